@@ -1,0 +1,299 @@
+#!/usr/bin/env python
+"""CBS steps/s on the 64^3 jittered lid-driven cavity (1,572,864 P1 tets,
+274,625 nodes, interior nodes jittered by U(-0.15h, 0.15h) from seed 1234,
+Re=400, local time step csafm=0.5, Jacobi-PCG to relative 1e-10).
+
+One "step" is one complete CBS step (time step, LHS, Steps 1-4, norms) on
+device-resident state.  The timed region holds K steps bracketed by a
+barrier and a device synchronise; time comes from CUDA events on the
+engine's stream (max over ranks).  Every step streams ~0.9 GB of element
+and node data, far more than the 126 MB L2, so no flush is inserted.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--precision fp64|mixed]
+  python bench.py --impl reference ...   # the reference solver on the host cores
+
+Multi-GPU: the single-case path does not shard (replicas only); each rank
+runs its own replica and `value` is the total steps/s of all ranks.
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "cbs-3d_b200"))
+sys.path.insert(0, ROOT)
+
+METRIC = "CBS steps/s, 64³ cavity: mixed vs FP64 GPU at ≤1e-8 rel err; PCG HBM GB/s"
+N_HEX, RE, JITTER, SEED = 64, 400.0, 0.15, 1234
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="gpu", choices=["gpu", "reference"])
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
+    ap.add_argument("--n", type=int, default=N_HEX, help="hexes per side")
+    ap.add_argument("--e2e-steps", type=int, default=3)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+def workload(n: int) -> str:
+    return (f"lid-driven cavity {n}^3 hexes x 6 Kuhn tets, interior jitter +-{JITTER}h seed {SEED}, "
+            f"Re={RE:g}, local dt csafm=0.5, Jacobi-PCG relTol 1e-10")
+
+
+def make_case(n: int, ntime: int):
+    from cbs3d import cases
+    return cases.cavity(n, re=RE, ntime=ntime, jitter=JITTER, seed=SEED)
+
+
+# ----------------------------------------------------------------- clocks
+class ClockSampler:
+    """nvidia-smi samples of SM clock and throttle reasons during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", "-i", str(device), f"--query-gpu={self.Q}",
+                                       "--format=csv,noheader,nounits", "-lms", "200"],
+                                      stdout=self.f, stderr=subprocess.DEVNULL)
+        except OSError:
+            self.p = None
+
+    def stop(self) -> dict:
+        if self.p is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.p.terminate()
+        try:
+            self.p.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.p.kill()
+        self.f.flush()
+        self.f.seek(0)
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.f:
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx.append(float(parts[2]))
+            except ValueError:
+                continue
+            for name, v in zip(names, parts[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(name)
+        os.unlink(self.f.name)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def measured_peak():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        with open(path) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def ncu_traffic(n: int):
+    """DRAM bytes per PCG launch from the committed ncu summary, if one exists
+    for this mesh size."""
+    path = os.path.join(ROOT, "profiles", "pcg_traffic.json")
+    if not os.path.exists(path):
+        return None
+    with open(path) as f:
+        d = json.load(f)
+    return d.get(str(n))
+
+
+# ----------------------------------------------------------- CPU baseline
+def reference_harness():
+    return os.path.join(ROOT, "oracle", "_ref", "cbs_ref_harness")
+
+
+def run_reference(case, steps: int, warmup: int, threads: int) -> dict:
+    with tempfile.TemporaryDirectory() as tmp:
+        base = case.write(tmp, "cavity")
+        env = dict(os.environ, OMP_NUM_THREADS=str(threads), OMP_PROC_BIND="close", OMP_PLACES="cores")
+        out = subprocess.run([reference_harness(), base, str(steps), tmp, "--time", "--warmup", str(warmup)],
+                             check=True, capture_output=True, text=True, env=env)
+    return json.loads(out.stdout.strip().splitlines()[-1])
+
+
+def cpu_baseline(n: int) -> dict:
+    threads = os.cpu_count() or 1
+    if not os.path.exists(reference_harness()):
+        return {"value": None, "unit": "steps/s", "cores": threads, "kind": "reference",
+                "sample": "unavailable: oracle/_ref/cbs_ref_harness not built"}
+    case = make_case(n, ntime=2)
+    r = run_reference(case, steps=1, warmup=0, threads=threads)
+    return {"value": r["steps_per_s"], "unit": "steps/s", "cores": r["threads"], "kind": "reference",
+            "sample": f"first CBS step of the same {n}^3 cavity ({r['last_cg_iterations']} PCG iterations), "
+                      f"reference compiled from its sources, OpenMP {r['threads']} threads, "
+                      f"{r['seconds']:.1f} s"}
+
+
+# ----------------------------------------------------------------- arms
+def dist_init():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    dist = None
+    if ws > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group(backend="nccl", timeout=datetime.timedelta(seconds=120))
+    return ws, rank, local, dist
+
+
+def dist_max(dist, x: float) -> float:
+    if dist is None:
+        return x
+    import torch
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(dist):
+    if dist is not None:
+        dist.barrier()
+
+
+def arm_reference(args):
+    ws, rank, _, dist = dist_init()
+    if rank != 0:
+        barrier(dist)
+        if dist is not None:
+            dist.destroy_process_group()
+        return
+    case = make_case(args.n, ntime=10 ** 6)
+    threads = os.cpu_count() or 1
+    k = max(1, min(args.steps, 2))
+    w = min(args.warmup, 1)
+    if not os.path.exists(reference_harness()):
+        print(json.dumps({"impl": "reference", "unavailable": "reference harness oracle/_ref not built"}))
+    else:
+        r = run_reference(case, steps=k, warmup=w, threads=threads)
+        v = r["steps_per_s"]
+        print(json.dumps({
+            "impl": "reference", "metric": METRIC, "value": v, "unit": "steps/s", "n_gpus": ws,
+            "steps": r["steps"], "warmup": w, "ms_per_step": 1e3 / v, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": workload(args.n), "precision": "fp64", "parallelism": "host OpenMP"},
+            "cpu_baseline": {"value": v, "unit": "steps/s", "cores": r["threads"], "kind": "reference",
+                             "sample": f"{r['steps']} timed CBS steps after {w} warm-up step(s) of the same "
+                                       f"cavity; the reference's own OpenMP build ({r['threads']} threads)"},
+            "e2e": {"value": v, "unit": "steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        }))
+    barrier(dist)
+    if dist is not None:
+        dist.destroy_process_group()
+
+
+def arm_gpu(args):
+    from cbs3d import gpu
+    ws, rank, local, dist = dist_init()
+    prec = gpu.MIXED if args.precision == "mixed" else gpu.FP64
+    case = make_case(args.n, ntime=10 ** 6)
+    ctx = gpu.Context(case, precision=prec, device=local, use_graph=False, time_pcg=True)
+    N = ctx.npoin
+    warm = ctx.step(args.warmup)
+    clocks = ClockSampler(local)
+    barrier(dist)
+    st = ctx.step(args.steps)
+    barrier(dist)
+    sec = dist_max(dist, st.gpu_seconds)
+    clk = clocks.stop()
+    # PCG iterations inside the timed region (the totals are cumulative)
+    its_timed = st.cg_iterations_total - warm.cg_iterations_total
+    value = ws * args.steps / sec
+    peak, peak_kind = measured_peak()
+    bpi = st.pcg_bytes_per_iter
+    pcg_avg = st.pcg_seconds / max(st.pcg_launches, 1)
+    achieved = its_timed * bpi / st.pcg_seconds / 1e9 if st.pcg_seconds > 0 else None
+    traffic = ncu_traffic(args.n)
+
+    # end to end through the public API with host buffers: upload the state,
+    # one step, download the state, every step
+    e2e = None
+    if args.e2e_steps > 0:
+        import torch
+        pin = torch.empty(5 * N, dtype=torch.float64, pin_memory=True).numpy()
+        u, p, t = ctx.fields()
+        pin[:3 * N] = u
+        pin[3 * N:4 * N] = p
+        pin[4 * N:] = t
+        hu, hp, ht = pin[:3 * N], pin[3 * N:4 * N], pin[4 * N:]
+        barrier(dist)
+        t0 = time.perf_counter()
+        for _ in range(args.e2e_steps):
+            ctx.upload(hu, hp, ht)
+            ctx.step(1)
+            ctx._check(gpu.lib().cbs3d_download_fields(ctx.h, gpu._ptr(hu), gpu._ptr(hp), gpu._ptr(ht)))
+        el = dist_max(dist, time.perf_counter() - t0)
+        e2e = {"value": ws * args.e2e_steps / el, "unit": "steps/s", "h2d_bytes_per_step": 5 * N * 8,
+               "d2h_bytes_per_step": 5 * N * 8}
+
+    cpu = None
+    if rank == 0 and ws == 1 and not args.no_cpu_baseline:
+        cpu = cpu_baseline(args.n)
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": "steps/s", "n_gpus": ws, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": 1e3 * sec / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64" if prec == gpu.FP64 else "f32+f64",
+            "data": "synthetic",
+            "config": {"workload": workload(args.n), "nelem": ctx.nelem, "npoin": N,
+                       "precision": args.precision, "l2": "inputs larger than L2 (no flush)",
+                       "parallelism": "replicas" if ws > 1 else "single"},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak if achieved else None, "traffic": traffic,
+                         "kernel": "k_pcg64 (persistent PCG solve)", "peak_source": peak_kind,
+                         "bytes_per_iteration": bpi, "iterations": its_timed, "launches": st.pcg_launches,
+                         "avg_launch_ms": 1e3 * pcg_avg},
+            "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": int(st.kernel_launches), "clocks": clk,
+            "pcg_iterations_per_step": its_timed / args.steps,
+            "pcg_share_of_step": st.pcg_seconds / st.gpu_seconds if st.gpu_seconds > 0 else None,
+        }
+        print(json.dumps(line))
+    ctx.close()
+    if dist is not None:
+        barrier(dist)
+        dist.destroy_process_group()
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        arm_reference(args)
+    else:
+        arm_gpu(args)
+
+
+if __name__ == "__main__":
+    main()

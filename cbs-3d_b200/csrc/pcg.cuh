@@ -1,0 +1,92 @@
+// Pressure PCG engine: the element-by-element pressure operator assembled per
+// step into a SELL-32 row layout, and a persistent cooperative Jacobi-PCG
+// kernel that runs a whole solve in one launch.
+#pragma once
+
+#include "dev_state.cuh"
+#include "host_model.h"
+
+#include <cuda_runtime.h>
+#include <vector>
+
+namespace cbs3d {
+
+struct CgOut {
+    int iterations;
+    int converged;
+    int outer;
+    int pad;
+    double initial_l2, final_l2, rel, max_abs;
+};
+
+struct PcgDev {
+    int N, E, nslices;
+    int nblocks;
+    int precond, conv_test, max_iter;
+    double rel_tol, abs_tol, inner_tol;
+    const long long* slice_off;
+    const int* slice_w;
+    const int* col;
+    double* val;
+    float* val32;
+    const long long* cptr;
+    const int* cent;
+    const uint8_t* nflag;        // bit0 pressure-active (touches fluid), bit2 fixed
+    const double* pfix;
+    double *pres, *rhs1, *pdiag;
+    double *r, *z, *pA, *pB, *q;
+    float *r32, *z32, *pA32, *pB32, *q32, *x32, *dinv32;
+    double* part;                // nblocks * 8
+    unsigned* bar;               // [0] count, [1] generation
+    DevStatus* status;
+    CgOut* out;
+};
+
+// Owns the device copies of the pattern and the PCG work vectors.
+class PcgEngine {
+public:
+    void init(const HostModel& m, const uint8_t* d_nflag, const double* d_pfix, DevStatus* d_status,
+              int device, int blocks_override, bool mixed);
+    void release();
+    // ELL values from gstifE*delte (step path) or from a caller's gstif[6E].
+    void assemble_from_state(const DevState& S, cudaStream_t st);
+    void assemble_from_gstif(const double* d_gstif, cudaStream_t st);
+    // Runs one solve on pres/rhs1/pdiag (device pointers), result to host.
+    // ev0/ev1 (optional) are recorded around the persistent PCG launch.
+    cbs3d_status solve(double* d_pres, double* d_rhs1, double* d_pdiag, int precond, int conv_test,
+                       int max_iter, double rel_tol, double abs_tol, cudaStream_t st, bool sync,
+                       cudaEvent_t ev0 = nullptr, cudaEvent_t ev1 = nullptr);
+    int extra_launches_per_solve() const { return 0; }
+    cbs3d_status read_result(cbs3d_cg_result& r, cudaStream_t st);
+    // y = A x with the assembled operator (identity rows on fixed nodes).
+    void multiply(const double* d_pdiag, const double* d_x, double* d_y, cudaStream_t st);
+
+    bool mixed = false;
+    double inner_tol = 1.0e-5;
+    int N = 0, E = 0, nslices = 0, nblocks = 0;
+    long long nslots = 0, ncontrib = 0;
+    long long *d_slice_off = nullptr, *d_cptr = nullptr;
+    int *d_slice_w = nullptr, *d_col = nullptr, *d_cent = nullptr;
+    double* d_val = nullptr;
+    float* d_val32 = nullptr;
+    double *d_r = nullptr, *d_z = nullptr, *d_pA = nullptr, *d_pB = nullptr, *d_q = nullptr;
+    float *d_f32 = nullptr;
+    double* d_part = nullptr;
+    unsigned* d_bar = nullptr;
+    CgOut* d_out = nullptr;
+    const uint8_t* d_nflag = nullptr;
+    const double* d_pfix = nullptr;
+    DevStatus* d_status = nullptr;
+    PcgDev dev{};
+    // Algorithmic bytes of one PCG iteration of the implemented kernel: the
+    // real (unpadded) pair coefficients and columns plus the per-node vector
+    // traffic of the two phases.
+    size_t bytes_per_iter() const;
+    long long nnz_offdiag = 0;
+};
+
+// Launches a grid whose barrier can never complete and reports the status
+// the bounded waits recorded (CBS3D_TIMEOUT when they ran out as designed).
+cbs3d_status selftest_wait_timeout(int device, int* observed);
+
+}  // namespace cbs3d

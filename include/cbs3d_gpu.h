@@ -1,0 +1,217 @@
+/*
+ * cbs3d_gpu.h - C ABI of the B200 CBS3D step engine.
+ *
+ * Plain pointers and sizes only; no exceptions cross this boundary.  Every
+ * call returns a cbs3d_status; cbs3d_last_error() gives the message, worded
+ * like the reference's std::runtime_error text where one exists.
+ *
+ * Host arrays follow the reference's storage order with the unused 1-based
+ * slot removed (a reference caller passes Array.raw().data() + 1):
+ *   intma[4*nelem]   element-major, 1-based node ids
+ *   coord[3*npoin]   node-major x,y,z          unkno[3*npoin] node-major u,v,w
+ *   gstif[6*nelem]   pair order 12,13,14,23,24,34
+ *   bface[5*nboun]   n1 n2 n3 parent_element solver_bc   (1-based ids)
+ *
+ * One context owns one CUDA stream and its device memory; a context is not
+ * thread-safe, separate contexts are independent.
+ */
+#ifndef CBS3D_GPU_H
+#define CBS3D_GPU_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum cbs3d_status {
+    CBS3D_OK = 0,
+    CBS3D_INVALID_INPUT = 1,   /* bad mesh/parameter/state (reference: runtime_error) */
+    CBS3D_NOT_CONVERGED = 2,   /* pressure PCG hit cg_max_iter */
+    CBS3D_BREAKDOWN = 3,       /* PCG pAp or r.z dot product invalid */
+    CBS3D_NONFINITE = 4,       /* NaN/Inf met in a field or residual */
+    CBS3D_TIMEOUT = 5,         /* a device-side wait ran out of its spin limit */
+    CBS3D_CUDA_ERROR = 6,
+    CBS3D_IO_ERROR = 7,        /* case file missing or malformed */
+    CBS3D_INTERNAL = 8
+} cbs3d_status;
+
+typedef enum cbs3d_precision {
+    CBS3D_FP64 = 0,            /* every stage in FP64 (parity form) */
+    CBS3D_MIXED = 1            /* FP32 inner PCG with FP64 residual correction */
+} cbs3d_precision;
+
+/* Run configuration: the RunConfig fields read by the step path
+ * (reference include/cbs/core/RunConfig.hpp:38-323), as parsed from .par. */
+typedef struct cbs3d_params {
+    int solver_opt, restart_opt, temp_calc;
+    double cinf[5];                               /* Ux Uy Uz P T */
+    int ntime, transient_on, dtfixed;
+    double dtfix;
+    int iwrite;
+    double csafm, theta1;
+    int cbs_scheme, ilots, htype, step2_check, rem_deltp, beta_opt, dtfix_end;
+    double csafm2, epsilon1, deltr;
+    double re, pr, ra, ri;
+    int convection_type, pnode;
+    int write_output;
+    double write_time_output, time_output_interval, end_rtime;
+    double relToler, absToler;
+    int vel_check;
+    double l2norm_vel_tolerance;
+    int temp_check;
+    double l2norm_temp_tolerance;
+    int paraview_output, tecplot_output, nusselt_calc, nusselt_flag, runtime_mod;
+    double alpha_sf, k_ratio, source_solid, heat_flux_bc;
+    int dimensional_mode, material_properties_enabled, mass_flow_inlet_enabled;
+    double p_ref, model_depth, inlet_mass_flow_rate, inlet_density, inlet_temperature,
+           outlet_pressure_gauge;
+    double inlet_u, inlet_v, inlet_w;
+    double nusselt_Tinf, nusselt_Tref, nusselt_diameter;
+    int cg_preconditioner, cg_conv_test, cg_max_iter;
+    double l2norm_pres_tolerance;
+    int residual_log_enabled, residual_log_every, console_log_every, live_residual_plot,
+        vtu_output_enabled, vtu_output_every_iterations;
+    double vtu_output_every_sim_time;
+    int write_boundary_debug_arrays, steady_min_iterations, art_diff;
+} cbs3d_params;
+
+/* Mesh in the reference layout after .bco mapping.  The property arrays are
+ * per element and are read only when material_properties_enabled > 0. */
+typedef struct cbs3d_mesh {
+    int nelem, npoin, nboun;
+    const int* intma;
+    const double* coord;
+    const int* bface;
+    const int* mat_elem;                           /* may be NULL: all fluid */
+    const double *rho, *cp, *k, *mu, *qvol;        /* may be NULL */
+} cbs3d_mesh;
+
+typedef struct cbs3d_options {
+    int precision;           /* cbs3d_precision */
+    int device;              /* CUDA device ordinal */
+    double inner_tol;        /* MIXED: relative FP32 inner tolerance (default 1e-5) */
+    int use_graph;           /* capture the per-step launch sequence in a CUDA graph */
+    int pcg_blocks;          /* persistent PCG grid size; 0 = one wave of resident CTAs */
+    int verbose;
+    int time_pcg;            /* time every PCG launch with CUDA events (no graph capture) */
+} cbs3d_options;
+
+/* Mirrors ConjugateGradient::Result (include/cbs/linalg/ConjugateGradient.hpp:36-68).
+ * Timings are GPU-event times of the solve; the reference's per-part timers
+ * have no separate counterpart inside the fused kernel and stay 0. */
+typedef struct cbs3d_cg_result {
+    int iterations;
+    double initial_l2, final_l2, final_relative_l2, final_max_abs;
+    int converged;
+    double total_seconds, setup_seconds, matvec_seconds, dot_seconds,
+           preconditioner_seconds, vector_update_seconds, constraint_seconds;
+    int matvec_calls, dot_calls, preconditioner_calls;
+    int outer_sweeps;        /* MIXED: FP64 residual corrections performed */
+} cbs3d_cg_result;
+
+typedef struct cbs3d_step_stats {
+    int steps_done;          /* steps completed by this call */
+    int iitime;              /* global step counter after the call */
+    int failed_step;         /* step at which a failure was detected, else 0 */
+    double dtreal;           /* last step's global minimum time step */
+    double rtime;            /* accumulated physical time (transient runs) */
+    cbs3d_cg_result cg;      /* last step's pressure solve */
+    long long cg_iterations_total;
+    double hb[15];           /* Convergence::evaluate measures of the last step */
+    double gpu_seconds;      /* device time of the steps of this call */
+    int steady_reached;      /* Convergence::steadyStateReached at the last step */
+    double pcg_seconds;      /* with time_pcg: summed duration of the PCG kernel launches */
+    int pcg_launches;        /* with time_pcg: PCG kernel launches timed */
+    long long kernel_launches; /* kernels this library launched during the call */
+    double pcg_bytes_per_iter; /* algorithmic bytes of one PCG iteration (see PCG roofline) */
+} cbs3d_step_stats;
+
+typedef struct cbs3d_ctx cbs3d_ctx;
+typedef struct cbs3d_pcg cbs3d_pcg;
+
+int cbs3d_version(void);
+const char* cbs3d_status_string(cbs3d_status s);
+void cbs3d_default_options(cbs3d_options* opt);
+void cbs3d_default_params(cbs3d_params* p);
+
+/* Parses <case>.par/.plt/.bco[/.material/.matprop] with the grammar of
+ * MeshIO::readAll (reference src/io/MeshIO.cpp:572-1701) into caller-visible
+ * sizes and parameters.  Replaces MeshIO::readSizes/readParameterFile. */
+cbs3d_status cbs3d_read_params(const char* case_name, cbs3d_params* params,
+                               int* nelem, int* npoin, int* nboun, char* err, size_t errlen);
+
+/* Reads the case files and builds a device context: replaces MeshIO::readAll
+ * + Solver::initialise + Solver::preparePressureSystem
+ * (reference src/solver/Solver.cpp:242-302, 587-593). */
+cbs3d_status cbs3d_create_from_case(const char* case_name, const cbs3d_options* opt,
+                                    cbs3d_ctx** out, char* err, size_t errlen);
+
+/* Same from in-memory arrays (raw side ids already mapped to solver BCs).
+ * Applies MeshIO::initialiseFields (src/io/MeshIO.cpp:1627-1701). */
+cbs3d_status cbs3d_create(const cbs3d_mesh* mesh, const cbs3d_params* params,
+                          const cbs3d_options* opt, cbs3d_ctx** out, char* err, size_t errlen);
+
+void cbs3d_destroy(cbs3d_ctx* ctx);
+const char* cbs3d_last_error(const cbs3d_ctx* ctx);
+
+/* Advances nsteps CBS steps, each replacing Solver::advanceOneStep
+ * (reference src/solver/Solver.cpp:609-680): TimeStep::computeTimeStep,
+ * updateLhsDiagonal, Steps::step1..step4, updateVelocityMagnitude and
+ * Convergence::evaluate, all on the device.  Stops early with
+ * stop_on_steady != 0 once Solver::steadyStateReached would stop the
+ * reference loop (src/solver/Solver.cpp:197-203, 708-716). */
+cbs3d_status cbs3d_step(cbs3d_ctx* ctx, int nsteps, int stop_on_steady, cbs3d_step_stats* stats);
+
+/* Field transfer (node-major, npoin entries per scalar).  NULL skips a field. */
+cbs3d_status cbs3d_upload_fields(cbs3d_ctx* ctx, const double* unkno, const double* pres,
+                                 const double* temperature);
+cbs3d_status cbs3d_download_fields(cbs3d_ctx* ctx, double* unkno, double* pres,
+                                   double* temperature);
+
+/* Named state access for stage-level checks (names follow CBSStateSI:
+ * unkno unkn1 pres pres1 temperature temperature1 rhs rhs1 delte elcoe2
+ * elcoe2p pdiag gstif detJ dNkdx annxf alen_e pdiagE gstifE velocity dtreal
+ * hb ncolor color_ptr color_elem bc_list wall_node_list fedge iside).
+ * count is the caller's capacity in elements; *written receives the size. */
+cbs3d_status cbs3d_get_array(cbs3d_ctx* ctx, const char* name, void* host, long count, long* written);
+cbs3d_status cbs3d_set_array(cbs3d_ctx* ctx, const char* name, const void* host, long count);
+
+/* Runs one named stage of a step on the device: begin_step, time_step, lhs,
+ * step1, step2_rhs, solve_pressure, step3, step4, convergence. */
+cbs3d_status cbs3d_run_stage(cbs3d_ctx* ctx, const char* stage);
+
+/* y = A x with the context's current pressure operator
+ * (MatrixVectorCalc::pressureMultiply, src/linalg/MatrixVectorCalc.cpp:125-205). */
+cbs3d_status cbs3d_pressure_multiply(cbs3d_ctx* ctx, const double* x, double* y);
+
+/* ---------------------------------------------------------------------------
+ * Pressure-solver drop-in: a solver_opt backend with the inputs and side
+ * effects of ConjugateGradient::solvePressure(CBSStateSI&)
+ * (reference src/linalg/ConjugateGradient.cpp:584-869; dispatch at
+ * src/solver/Steps.cpp:305-350).  Create once after preprocessing, solve
+ * every step.
+ * --------------------------------------------------------------------------- */
+cbs3d_status cbs3d_pcg_create(int nelem, int npoin, const int* intma, const int* mat_elem,
+                              int bc_fixed, const int* bc_list, const double* bc_values,
+                              const cbs3d_options* opt, cbs3d_pcg** out, char* err, size_t errlen);
+
+/* pres: initial guess in, solution out.  rhs1 and pdiag are overwritten on
+ * fixed and inactive nodes exactly as impose_pressure_constraints does. */
+cbs3d_status cbs3d_pcg_solve(cbs3d_pcg* pcg, int cg_preconditioner, int cg_conv_test,
+                             int cg_max_iter, double relToler, double absToler,
+                             const double* gstif, double* pdiag, double* rhs1, double* pres,
+                             cbs3d_cg_result* result);
+void cbs3d_pcg_destroy(cbs3d_pcg* pcg);
+const char* cbs3d_pcg_last_error(const cbs3d_pcg* pcg);
+
+/* Failure-detection self-test (no reference counterpart): launches a small
+ * grid whose grid barrier can never complete and returns, in
+ * *observed_status, the status its bounded device waits recorded --
+ * CBS3D_TIMEOUT after about a second.  The device stays usable. */
+cbs3d_status cbs3d_selftest_wait_timeout(int device, int* observed_status);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -773,7 +773,7 @@ int orc_time_step(orc_state* s, int iitime)
 }
 
 /* TimeStep::applyStep2PressureTimeStepCorrection, src/timestep/TimeStep.cpp:704-749 */
-static int step2_dt_correction(orc_state* s)
+int orc_dt_correction(orc_state* s)
 {
     if (s->p.step2_check < 1) return 0;
     if (s->p.csafm2 <= 0.0 || !isfinite(s->p.csafm2)) return fail(s, "TimeStep::applyStep2PressureTimeStepCorrection - csafm2 must be positive");
@@ -1264,7 +1264,7 @@ int orc_step(orc_state* s, int iitime)
     if (orc_lhs(s)) return 1;
     if (orc_step1(s)) return 1;
     if (s->p.step2_check > 0) {
-        if (step2_dt_correction(s)) return 1;
+        if (orc_dt_correction(s)) return 1;
         if (orc_lhs(s)) return 1;
     }
     if (orc_step2_rhs(s)) return 1;

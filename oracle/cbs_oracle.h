@@ -60,6 +60,7 @@ int orc_begin_step(orc_state* s);                 /* unkn1=unkno, pres1=pres, T1
 int orc_time_step(orc_state* s, int iitime);      /* TimeStep::computeTimeStep */
 int orc_lhs(orc_state* s);                        /* TimeStep::updateLhsDiagonal */
 int orc_step1(orc_state* s);                      /* Steps::step1SemiImplicit */
+int orc_dt_correction(orc_state* s);              /* TimeStep::applyStep2PressureTimeStepCorrection */
 int orc_step2_rhs(orc_state* s);                  /* PressureAssembly::assembleStep2Rhs */
 int orc_solve_pressure(orc_state* s);             /* ConjugateGradient::solvePressure + applyPressure */
 int orc_step3(orc_state* s);                      /* Steps::step3SemiImplicit */

@@ -55,7 +55,7 @@ def lib():
         for fn in ("orc_step", "orc_time_step"):
             getattr(L, fn).argtypes = [ctypes.c_void_p, ctypes.c_int]
             getattr(L, fn).restype = ctypes.c_int
-        for fn in ("orc_begin_step", "orc_lhs", "orc_step1", "orc_step2_rhs", "orc_solve_pressure",
+        for fn in ("orc_begin_step", "orc_lhs", "orc_step1", "orc_dt_correction", "orc_step2_rhs", "orc_solve_pressure",
                    "orc_step3", "orc_step4", "orc_convergence"):
             getattr(L, fn).argtypes = [ctypes.c_void_p]
             getattr(L, fn).restype = ctypes.c_int

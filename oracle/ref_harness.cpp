@@ -12,6 +12,7 @@
 //     --stage K   dump every intermediate array of step K (1-based)
 //     --every M   dump u/p/T after every M-th step
 //     --time      time the step loop only and print one JSON line
+//     --warmup W  with --time: run W untimed steps before the timed ones
 
 #include "cbs/assembly/EnergyAssembly.hpp"
 #include "cbs/assembly/MomentumAssembly.hpp"
@@ -240,13 +241,14 @@ int main(int argc, char** argv)
     const std::string case_name = argv[1];
     const int nsteps = std::atoi(argv[2]);
     g_out = argv[3];
-    int stage = 0, every = 0;
+    int stage = 0, every = 0, warmup = 0;
     bool timing = false;
     for (int i = 4; i < argc; ++i)
     {
         if (!std::strcmp(argv[i], "--stage") && i + 1 < argc) stage = std::atoi(argv[++i]);
         else if (!std::strcmp(argv[i], "--every") && i + 1 < argc) every = std::atoi(argv[++i]);
         else if (!std::strcmp(argv[i], "--time")) timing = true;
+        else if (!std::strcmp(argv[i], "--warmup") && i + 1 < argc) warmup = std::atoi(argv[++i]);
     }
 
     try
@@ -296,9 +298,12 @@ int main(int argc, char** argv)
 
         std::vector<Real> hist;
         StepRecord rec{};
+        Int it0 = 1;
+        if (timing)
+            for (; it0 <= warmup; ++it0) advance(s, it0, false, rec);
         const auto t0 = std::chrono::steady_clock::now();
         int done = 0;
-        for (Int it = 1; it <= nsteps; ++it)
+        for (Int it = it0; it < it0 + nsteps; ++it)
         {
             advance(s, it, !timing && it == stage, rec);
             ++done;

@@ -1,0 +1,179 @@
+"""GPU path against the reference's golden vectors and the oracle, through
+the C ABI (libcbs3d_gpu.so).
+
+Bitwise: preprocessing, colouring, BC lists, time step, LHS diagonals,
+Step 1, Step-2 RHS, the colour-ordered matvec, Step 3 and Step 4 (each stage
+fed the reference's inputs).  Tolerance: the PCG solve, whose dot products
+and assembled-operator sums run in a different (deterministic) order than
+the reference's serial loops -- every solve meets the reference's own
+stopping test ||r||/||r0|| <= relToler, and solutions agree to
+PCG_TOL relative L2; multi-step runs agree to RUN_TOL."""
+import json
+
+import numpy as np
+import pytest
+
+from helpers import STAGED, bitwise, fixture_path, load_case, rel_l2, stage_step
+
+pytestmark = pytest.mark.gpu
+
+PCG_TOL = 1e-8       # one pressure solve to relToler=1e-10, vs the reference's
+RUN_TOL = 1e-8       # short multi-step runs
+C1_TOL = 1e-10       # config-1 cavity after 500 steps (u, p)
+PRE = ["fedge", "detJ", "dNkdx", "annxf", "alen_e", "pdiagE", "gstifE", "color_ptr", "color_elem",
+       "bc_list", "bc_values", "wall_node_list", "face_norm", "iside"]
+
+
+def _gpu():
+    from cbs3d import gpu
+    return gpu
+
+
+def _ctx(name, **kw):
+    case, z = load_case(fixture_path(name))
+    return _gpu().Context(case, **kw), case, z
+
+
+def _param(z, key):
+    return json.loads(bytes(z["params_json"]).decode()).get(key, 0)
+
+
+@pytest.mark.parametrize("name", STAGED)
+def test_preprocess_bitwise(name):
+    c, _, z = _ctx(name)
+    for k in PRE:
+        assert bitwise(c.get(k), z["ref_" + k]), k
+    u, p, t = c.fields()
+    assert bitwise(u, z["ref_init_unkno"])
+    assert bitwise(p, z["ref_init_pres"])
+    assert bitwise(t, z["ref_init_temperature"])
+    assert bitwise(c.get("Mdiag_real"), z["ref_Mdiag_real"])
+
+
+@pytest.mark.parametrize("name", STAGED)
+def test_stages_bitwise(name):
+    c, _, z = _ctx(name)
+    k = stage_step(z)
+    for _ in range(k - 1):
+        c.stage("begin_step")   # advance the step counter only
+    c.upload(z["ref_s0_unkno"], z["ref_s0_pres"], z["ref_s0_temperature"])
+    c.stage("begin_step")
+    c.stage("time_step")
+    assert bitwise(c.get("delte"), z["ref_s1_delte"])
+    assert bitwise(c.get("dtreal"), z["ref_s1_dtreal"])
+    c.stage("lhs")
+    for a in ("elcoe2", "elcoe2p", "pdiag", "gstif", "pres"):
+        assert bitwise(c.get(a), z["ref_s2_" + a]), a
+    c.stage("step1")
+    assert bitwise(c.get("rhs"), z["ref_s3_rhs"])
+    assert bitwise(c.get("unkno"), z["ref_s3_unkno"])
+    if _param(z, "step2_check"):
+        c.stage("dt_correction")
+        c.stage("lhs")
+    c.stage("step2_rhs")
+    assert bitwise(c.get("rhs1"), z["ref_s4_rhs1"])
+    assert bitwise(c.get("pdiag"), z["ref_s4_pdiag_in"])
+    assert bitwise(c.get("gstif"), z["ref_s4_gstif"])
+    # MatrixVectorCalc::pressureMultiply in colour order
+    assert bitwise(c.pressure_multiply(z["ref_s4_pres_in"]), z["ref_s4_Apres"])
+    c.stage("solve_pressure")
+    cg = c.get("cg")
+    assert rel_l2(c.get("pres"), z["ref_s5_pres"]) <= PCG_TOL
+    assert abs(int(cg[0]) - int(z["ref_s5_cg"][0])) <= 2
+    assert bitwise(c.get("rhs1"), z["ref_s5_rhs1"])
+    assert bitwise(c.get("pdiag"), z["ref_s5_pdiag"])
+    # Step 3/4 from the reference's pressure
+    c.set("pres", z["ref_s5_pres"])
+    c.stage("step3")
+    assert bitwise(c.get("rhs"), z["ref_s6_rhs"])
+    assert bitwise(c.get("unkno"), z["ref_s6_unkno"])
+    c.stage("step4")
+    if "ref_s7_temperature" in z.files:
+        assert bitwise(c.get("rhs1"), z["ref_s7_rhs1"])
+        assert bitwise(c.get("temperature"), z["ref_s7_temperature"])
+    c.stage("convergence")
+    assert bitwise(c.get("velocity"), z["ref_s8_velocity"])
+    np.testing.assert_allclose(c.get("hb"), z["ref_s8_hb"], rtol=1e-12, atol=1e-300)
+
+
+@pytest.mark.parametrize("name", STAGED)
+def test_full_run(name):
+    c, _, z = _ctx(name)
+    n = int(z["nsteps"][0])
+    hist = z["ref_history"].reshape(n, 21)
+    for s in range(n):
+        st = c.step(1)
+        assert abs(st.cg.iterations - int(hist[s, 1])) <= 2
+        assert abs(st.dtreal - hist[s, 0]) <= 1e-12 * abs(hist[s, 0])
+    u, p, t = c.fields()
+    assert rel_l2(u, z["ref_final_unkno"]) <= RUN_TOL
+    assert rel_l2(p, z["ref_final_pres"]) <= RUN_TOL
+    if _param(z, "temp_calc") or _param(z, "material_enabled"):
+        assert rel_l2(t, z["ref_final_temperature"]) <= RUN_TOL
+
+
+def test_c1_cavity16_500_steps():
+    """Config 1: 16^3 x 6 Kuhn cavity, Re=100, local dt csafm=0.5,
+    Jacobi-PCG relTol 1e-10, 500 steps; u and p within 1e-10 relative L2 of
+    the reference after every 100 steps."""
+    c, _, z = _ctx("c1_cavity16")
+    hist = z["ref_history"].reshape(500, 21)
+    for blk in range(5):
+        st = c.step(100)
+        s = (blk + 1) * 100
+        u, p, _ = c.fields()
+        eu = rel_l2(u, z[f"ref_step{s}_unkno"])
+        ep = rel_l2(p, z[f"ref_step{s}_pres"])
+        print(f"step {s}: rel L2 u {eu:.3e} p {ep:.3e} cg {st.cg.iterations} (ref {int(hist[s - 1, 1])})")
+        assert eu <= C1_TOL and ep <= C1_TOL
+    assert abs(st.cg.iterations - int(hist[-1, 1])) <= 2
+
+
+def test_dropin_pressure_solver():
+    """cbs3d_pcg_solve with the reference's Step-2 inputs (solver_opt=1 drop-in)."""
+    case, z = load_case(fixture_path("cav6j"))
+    gpu = _gpu()
+    bc_list = z["ref_bc_list"]
+    ps = gpu.PressureSolver(case.mesh.intma, case.mesh.mat_elem, bc_list, z["ref_bc_values"])
+    pres, rhs1, pdiag, res = ps.solve(z["ref_s4_gstif"], z["ref_s4_pdiag_in"], z["ref_s4_rhs1"],
+                                      z["ref_s4_pres_in"], relToler=1e-10, absToler=1e-300)
+    assert res["status"] == 0 and res["converged"] == 1
+    assert rel_l2(pres, z["ref_s5_pres"]) <= PCG_TOL
+    assert bitwise(rhs1, z["ref_s5_rhs1"])
+    assert bitwise(pdiag, z["ref_s5_pdiag"])
+    assert abs(res["iterations"] - int(z["ref_s5_cg"][0])) <= 2
+    assert abs(res["initial_l2"] - z["ref_s5_cg"][1]) <= 1e-12 * abs(z["ref_s5_cg"][1])
+
+
+def test_deterministic_reruns():
+    a, _, _ = _ctx("cav6j")
+    b, _, _ = _ctx("cav6j")
+    a.step(5)
+    b.step(5)
+    for x, y in zip(a.fields(), b.fields()):
+        assert bitwise(x, y)
+
+
+def test_graph_and_eager_identical():
+    a, _, _ = _ctx("chan_sym", use_graph=True)
+    b, _, _ = _ctx("chan_sym", use_graph=False)
+    a.step(4)
+    b.step(4)
+    for x, y in zip(a.fields(), b.fields()):
+        assert bitwise(x, y)
+
+
+def test_case_files_contract(tmp_path):
+    """The engine's .plt/.bco/.par reader (cbs3d_create_from_case) against
+    the in-memory path on the same case."""
+    case, z = load_case(fixture_path("cht"))
+    base = case.write(str(tmp_path), "cht")
+    gpu = _gpu()
+    a = gpu.Context(case_name=base)
+    b = gpu.Context(case)
+    for k in ("detJ", "iside", "color_elem", "bc_list", "wall_node_list"):
+        assert bitwise(a.get(k), b.get(k)), k
+    a.step(3)
+    u, p, t = a.fields()
+    assert rel_l2(u, z["ref_final_unkno"]) <= RUN_TOL
+    assert rel_l2(t, z["ref_final_temperature"]) <= RUN_TOL

@@ -1,0 +1,83 @@
+"""Host-side checks that need no GPU: the C ABI library loads and exports
+every entry point of include/cbs3d_gpu.h, the case-file reader, and the
+synthetic case generator."""
+import ctypes
+import os
+import re
+
+import numpy as np
+import pytest
+
+from helpers import fixture_path, load_case
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def test_library_exports_header_symbols():
+    from cbs3d import gpu
+    L = gpu.lib()
+    hdr = open(os.path.join(ROOT, "include", "cbs3d_gpu.h")).read()
+    names = set(re.findall(r"\b(cbs3d_[a-z_0-9]+)\s*\(", hdr))
+    assert len(names) >= 20
+    for n in sorted(names):
+        assert hasattr(L, n), n
+
+
+def test_read_params_matches_generated_par(tmp_path):
+    from cbs3d import cases, gpu
+    c = cases.cht_slab(4, 2, 2, 2, ntime=7, q=2.5)
+    base = c.write(str(tmp_path), "x")
+    par = gpu.Params()
+    ne, npn, nb = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+    err = ctypes.create_string_buffer(512)
+    rc = gpu.lib().cbs3d_read_params(base.encode(), ctypes.byref(par), ctypes.byref(ne), ctypes.byref(npn),
+                                     ctypes.byref(nb), err, 512)
+    assert rc == 0, err.value
+    assert (ne.value, npn.value, nb.value) == (c.mesh.nelem, c.mesh.npoin, c.mesh.nboun)
+    assert par.ntime == 7 and par.heat_flux_bc == 2.5 and par.temp_calc == 1
+    assert par.material_properties_enabled == 1 and par.dimensional_mode == 1
+    assert par.re == 200.0 and par.relToler == 1e-10 and par.cg_conv_test == 2
+    assert par.steady_min_iterations == 7
+
+
+def test_missing_case_is_io_error(tmp_path):
+    from cbs3d import gpu
+    with pytest.raises(gpu.CBSError) as e:
+        gpu.Context(case_name=str(tmp_path / "nope"))
+    assert e.value.code == 7
+
+
+def test_unsupported_bco_id_rejected(tmp_path):
+    from cbs3d import cases, gpu
+    c = cases.cavity(2)
+    c.bc_map[1] = 777
+    base = c.write(str(tmp_path), "bad")
+    with pytest.raises(gpu.CBSError) as e:
+        gpu.Context(case_name=base)
+    assert e.value.code == 1
+    assert "unsupported solver BC ID 777" in e.value.message
+
+
+def test_generator_shapes_and_orientation():
+    from cbs3d import cases
+    for c in (cases.cavity(5, jitter=0.15, seed=3), cases.channel(6, 2, 3), cases.cht_slab(6, 3, 2, 2)):
+        m = c.mesh
+        x = m.coord[m.intma - 1]
+        v6 = np.einsum("ij,ij->i", x[:, 1] - x[:, 0], np.cross(x[:, 2] - x[:, 0], x[:, 3] - x[:, 0]))
+        assert np.all(v6 > 0)
+        nx, ny, nz = m.shape
+        assert m.nelem == 6 * nx * ny * nz
+        assert m.npoin == (nx + 1) * (ny + 1) * (nz + 1)
+        assert m.nboun == 4 * (nx * ny + ny * nz + nx * nz)
+
+
+def test_c2_sizes():
+    from cbs3d import cases
+    m = cases.box_mesh(64, 64, 64, jitter=0.15, seed=1234)
+    assert (m.nelem, m.npoin, m.nboun) == (1572864, 274625, 49152)
+
+
+def test_fixture_case_roundtrip():
+    case, z = load_case(fixture_path("cht"))
+    assert case.params["temp_calc"] == 1
+    assert case.mesh.nelem == int(z["ref_sizes"][0])
