@@ -205,6 +205,27 @@ cbs3d_status cbs3d_pcg_solve(cbs3d_pcg* pcg, int cg_preconditioner, int cg_conv_
 void cbs3d_pcg_destroy(cbs3d_pcg* pcg);
 const char* cbs3d_pcg_last_error(const cbs3d_pcg* pcg);
 
+/* Convergence measures without any device allocation (no counterpart in the
+ * reference): the 15 values of Convergence::evaluate, returned in hb, from
+ * device arrays the caller already holds (node-major unkno/unkn1[3*npoin],
+ * pres/pres1/temperature/temperature1/elcoe2/elcoe2p[npoin];
+ * node_flags[npoin]: bit0 = node touches a fluid element, bit1 = touches a
+ * solid element).  For callers that may not call cudaMalloc -- e.g. a host
+ * loop that must not stall the device or a process whose device memory is
+ * owned by another allocator: the only scratch is a 1 MiB file-scope device
+ * array that every GPU loading this library holds until exit.  npoin above
+ * 2,097,152 is rejected with CBS3D_INVALID_INPUT.  The first call on a device
+ * looks up that array's device address; make that first call before any
+ * stream capture.  All calls share the array: calls whose kernels overlap on
+ * the GPU race.  Runs on the legacy default stream and returns when hb is on
+ * the host. */
+cbs3d_status cbs3d_convergence_norms_static(int device, const double* unkno, const double* unkn1,
+                                            const double* pres, const double* pres1,
+                                            const double* temperature, const double* temperature1,
+                                            const double* elcoe2, const double* elcoe2p,
+                                            const unsigned char* node_flags, int npoin, int temp_calc,
+                                            double hb[15]);
+
 /* Failure-detection self-test (no reference counterpart): launches a small
  * grid whose grid barrier can never complete and returns, in
  * *observed_status, the status its bounded device waits recorded --
