@@ -79,7 +79,7 @@ class Mesh(ctypes.Structure):
 
 class Options(ctypes.Structure):
     _fields_ = [("precision", _i), ("device", _i), ("inner_tol", _d), ("use_graph", _i),
-                ("pcg_blocks", _i), ("verbose", _i), ("time_pcg", _i)]
+                ("pcg_blocks", _i), ("verbose", _i), ("time_pcg", _i), ("pcg_kernel", _i)]
 
 
 class CGResult(ctypes.Structure):
@@ -177,7 +177,7 @@ def make_params(p: dict) -> Params:
 
 
 def make_options(precision: int = FP64, device: int = 0, inner_tol: float = 1e-5, use_graph: bool = True,
-                 pcg_blocks: int = 0, time_pcg: bool = False) -> Options:
+                 pcg_blocks: int = 0, time_pcg: bool = False, pcg_kernel: int = 0) -> Options:
     o = Options()
     lib().cbs3d_default_options(ctypes.byref(o))
     o.precision = precision
@@ -186,6 +186,7 @@ def make_options(precision: int = FP64, device: int = 0, inner_tol: float = 1e-5
     o.use_graph = 1 if use_graph else 0
     o.pcg_blocks = pcg_blocks
     o.time_pcg = 1 if time_pcg else 0
+    o.pcg_kernel = pcg_kernel
     return o
 
 
@@ -193,11 +194,12 @@ class Context:
     """One case resident on the GPU."""
 
     def __init__(self, case=None, case_name: str | None = None, precision: int = FP64, device: int = 0,
-                 inner_tol: float = 1e-5, use_graph: bool = True, pcg_blocks: int = 0, time_pcg: bool = False):
+                 inner_tol: float = 1e-5, use_graph: bool = True, pcg_blocks: int = 0, time_pcg: bool = False,
+                 pcg_kernel: int = 0):
         L = lib()
         self.h = ctypes.c_void_p()
         err = ctypes.create_string_buffer(1024)
-        opt = make_options(precision, device, inner_tol, use_graph, pcg_blocks, time_pcg)
+        opt = make_options(precision, device, inner_tol, use_graph, pcg_blocks, time_pcg, pcg_kernel)
         if case_name is not None:
             rc = L.cbs3d_create_from_case(case_name.encode(), ctypes.byref(opt), ctypes.byref(self.h), err, 1024)
         else:

@@ -274,7 +274,7 @@ void cbs3d_ctx::setup()
     CUDA_OK(cudaStreamSynchronize(st));
     check_status();
     pcg.inner_tol = opt.inner_tol > 0.0 ? opt.inner_tol : 1.0e-5;
-    pcg.init(m, S.nflag, S.pfix, S.status, opt.device, opt.pcg_blocks, opt.precision == CBS3D_MIXED);
+    pcg.init(m, S.nflag, S.pfix, S.status, opt.device, opt.pcg_blocks, opt.precision == CBS3D_MIXED, opt.pcg_kernel);
 }
 
 void cbs3d_ctx::check_status()
@@ -867,7 +867,7 @@ cbs3d_status cbs3d_pcg_create(int nelem, int npoin, const int* intma, const int*
         p->d_pdiag = p->buf.alloc<double>(N);
         p->eng.inner_tol = p->opt.inner_tol > 0.0 ? p->opt.inner_tol : 1.0e-5;
         p->eng.init(m, p->d_nflag, p->d_pfix, p->d_status, p->opt.device, p->opt.pcg_blocks,
-                    p->opt.precision == CBS3D_MIXED);
+                    p->opt.precision == CBS3D_MIXED, p->opt.pcg_kernel);
         *out = p.release();
         return CBS3D_OK;
     } catch (const Error& e) {

@@ -21,8 +21,10 @@
 // CTAs and reproducible run to run.
 #include "pcg.cuh"
 
+#include <algorithm>
 #include <cstdio>
 #include <cstring>
+#include <vector>
 
 namespace cbs3d {
 
@@ -106,38 +108,61 @@ struct Acc4 {
     double a, b, mx, flag;
 };
 
-// Block partial of (sum a, sum b, max mx, max flag), written by thread 0 in
-// a fixed warp order.
-__device__ __forceinline__ void block_partial(Acc4 v, double* out)
+// Grid-wide all-reduce of (sum a, sum b, max mx, max flag) fused with the
+// grid barrier.  Each CTA stores its partial and arrives on a counter
+// (release); the CTA that arrives last reduces all partials in a fixed tree
+// -- the same tree whichever CTA it is, so the totals are deterministic --
+// publishes them and bumps the generation (release).  The others wait for the
+// generation (acquire, bounded by the spin limit of grid_barrier) and read the
+// totals.  One partial read per CTA instead of every CTA reading all partials.
+__device__ __forceinline__ bool grid_allreduce(Acc4 v, const PcgDev& D, int phase, Acc4& out)
 {
     __shared__ double sm[PCG_WARPS][4];
+    __shared__ double tot[4];
+    __shared__ int s_last, s_ok;
+    const int G = gridDim.x;
     for (int o = 16; o > 0; o >>= 1) {
         v.a += __shfl_down_sync(0xffffffffu, v.a, o);
         v.b += __shfl_down_sync(0xffffffffu, v.b, o);
         v.mx = fmax(v.mx, __shfl_down_sync(0xffffffffu, v.mx, o));
         v.flag = fmax(v.flag, __shfl_down_sync(0xffffffffu, v.flag, o));
     }
-    const int w = threadIdx.x >> 5;
-    if ((threadIdx.x & 31) == 0) { sm[w][0] = v.a; sm[w][1] = v.b; sm[w][2] = v.mx; sm[w][3] = v.flag; }
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    if (lane == 0) { sm[w][0] = v.a; sm[w][1] = v.b; sm[w][2] = v.mx; sm[w][3] = v.flag; }
     __syncthreads();
+    unsigned* cnt = D.bar;
+    unsigned* gen = D.bar + 1;
+    double* totals = D.part + (size_t)G * 4 + (size_t)(phase & 1) * 4;
     if (threadIdx.x == 0) {
         double a = 0.0, b = 0.0, mx = 0.0, fl = 0.0;
         for (int k = 0; k < PCG_WARPS; ++k) { a += sm[k][0]; b += sm[k][1]; mx = fmax(mx, sm[k][2]); fl = fmax(fl, sm[k][3]); }
-        out[0] = a; out[1] = b; out[2] = mx; out[3] = fl;
-        __threadfence();
+        double* p = D.part + (size_t)blockIdx.x * 4;
+        __stcg(p, a); __stcg(p + 1, b); __stcg(p + 2, mx); __stcg(p + 3, fl);
+        const unsigned g = ld_acquire(gen);
+        unsigned arrived;
+        asm volatile("atom.add.acq_rel.gpu.global.u32 %0, [%1], 1;" : "=r"(arrived) : "l"(cnt) : "memory");
+        s_last = (arrived == (unsigned)G - 1) ? 1 : 0;
+        s_ok = 1;
+        if (!s_last) {
+            const long long t0 = clock64();
+            while (ld_acquire(gen) == g) {
+                if (ld_relaxed_int(&D.status->code) != 0) { s_ok = 0; break; }
+                if (clock64() - t0 > (1LL << 31)) {
+                    set_status(D.status, 5 /*CBS3D_TIMEOUT*/, ST_PCG, 0, R_PCG_BARRIER);
+                    s_ok = 0;
+                    break;
+                }
+                __nanosleep(20);
+            }
+            if (s_ok) { tot[0] = __ldcg(totals); tot[1] = __ldcg(totals + 1); tot[2] = __ldcg(totals + 2); tot[3] = __ldcg(totals + 3); }
+        }
     }
-}
-
-// Grid total of the block partials, summed in the same fixed tree by every
-// CTA (lane l takes partials l, l+32, ... then a shuffle tree), so every CTA
-// obtains bit-identical totals.
-__device__ __forceinline__ Acc4 grid_total(const double* part, int G)
-{
-    __shared__ double tot[4];
-    if (threadIdx.x < 32) {
+    __syncthreads();
+    if (s_last) {
+        // fixed tree over the G partials: thread t takes t, t+T, ...; then warps; then thread 0
         double a = 0.0, b = 0.0, mx = 0.0, fl = 0.0;
-        for (int k = threadIdx.x; k < G; k += 32) {
-            const double* p = part + (size_t)k * 8;
+        for (int k = threadIdx.x; k < G; k += PCG_THREADS) {
+            const double* p = D.part + (size_t)k * 4;
             a += __ldcg(p); b += __ldcg(p + 1); mx = fmax(mx, __ldcg(p + 2)); fl = fmax(fl, __ldcg(p + 3));
         }
         for (int o = 16; o > 0; o >>= 1) {
@@ -146,12 +171,24 @@ __device__ __forceinline__ Acc4 grid_total(const double* part, int G)
             mx = fmax(mx, __shfl_down_sync(0xffffffffu, mx, o));
             fl = fmax(fl, __shfl_down_sync(0xffffffffu, fl, o));
         }
-        if (threadIdx.x == 0) { tot[0] = a; tot[1] = b; tot[2] = mx; tot[3] = fl; }
+        __syncthreads();
+        if (lane == 0) { sm[w][0] = a; sm[w][1] = b; sm[w][2] = mx; sm[w][3] = fl; }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            double ta = 0.0, tb = 0.0, tm = 0.0, tf = 0.0;
+            for (int k = 0; k < PCG_WARPS; ++k) { ta += sm[k][0]; tb += sm[k][1]; tm = fmax(tm, sm[k][2]); tf = fmax(tf, sm[k][3]); }
+            tot[0] = ta; tot[1] = tb; tot[2] = tm; tot[3] = tf;
+            __stcg(totals, ta); __stcg(totals + 1, tb); __stcg(totals + 2, tm); __stcg(totals + 3, tf);
+            atomicExch(cnt, 0u);
+            asm volatile("red.release.gpu.global.add.u32 [%0], 1;" :: "l"(gen) : "memory");
+            if (ld_relaxed_int(&D.status->code) != 0) s_ok = 0;
+        }
     }
     __syncthreads();
-    Acc4 r{tot[0], tot[1], tot[2], tot[3]};
+    out = Acc4{tot[0], tot[1], tot[2], tot[3]};
+    const bool ok = s_ok != 0;
     __syncthreads();
-    return r;
+    return ok;
 }
 
 __device__ __forceinline__ bool cg_converged(int test, double rel, double mx, double rtol, double atol)
@@ -181,8 +218,6 @@ __global__ void __launch_bounds__(PCG_THREADS) k_pcg64(PcgDev D)
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int s_beg = (int)((long long)b * D.nslices / G);
     const int s_end = (int)((long long)(b + 1) * D.nslices / G);
-    unsigned* cnt = D.bar;
-    unsigned* gen = D.bar + 1;
     int phase = 0;
     const int N = D.N;
 
@@ -218,9 +253,8 @@ __global__ void __launch_bounds__(PCG_THREADS) k_pcg64(PcgDev D)
         D.z[i] = zi;
         D.pA[i] = zi;
     }
-    block_partial(acc, D.part + ((size_t)(phase & 1) * G + b) * 8);
-    if (!grid_barrier(cnt, gen, G, D.status, ST_PCG)) return;
-    Acc4 t = grid_total(D.part + (size_t)(phase & 1) * G * 8, G);
+    Acc4 t = Acc4{0.0, 0.0, 0.0, 0.0};
+    if (!grid_allreduce(acc, D, phase, t)) return;
     ++phase;
     const double init = sqrt(t.a);
     if (init <= 1.0e-300) { cg_finish(D, 0, 1, init, init, 0.0, t.mx); return; }
@@ -261,9 +295,8 @@ __global__ void __launch_bounds__(PCG_THREADS) k_pcg64(PcgDev D)
             D.q[i] = qi;
             if (freen) pa.a = fma(pci, qi, pa.a);
         }
-        block_partial(pa, D.part + ((size_t)(phase & 1) * G + b) * 8);
-        if (!grid_barrier(cnt, gen, G, D.status, ST_PCG)) return;
-        t = grid_total(D.part + (size_t)(phase & 1) * G * 8, G);
+        t = Acc4{0.0, 0.0, 0.0, 0.0};
+        if (!grid_allreduce(pa, D, phase, t)) return;
         ++phase;
         const double pAp = t.a;
         if (fabs(pAp) <= 1.0e-300 || !isfinite(pAp)) { if (b == 0 && threadIdx.x == 0) set_status(D.status, 3, ST_PCG, it, R_PCG_PAP); return; }
@@ -286,9 +319,8 @@ __global__ void __launch_bounds__(PCG_THREADS) k_pcg64(PcgDev D)
             rr.b = fma(ri, zi, rr.b);
             rr.mx = fmax(rr.mx, fabs(ri));
         }
-        block_partial(rr, D.part + ((size_t)(phase & 1) * G + b) * 8);
-        if (!grid_barrier(cnt, gen, G, D.status, ST_PCG)) return;
-        t = grid_total(D.part + (size_t)(phase & 1) * G * 8, G);
+        t = Acc4{0.0, 0.0, 0.0, 0.0};
+        if (!grid_allreduce(rr, D, phase, t)) return;
         ++phase;
         fin = sqrt(t.a);
         mx = t.mx;
@@ -300,6 +332,363 @@ __global__ void __launch_bounds__(PCG_THREADS) k_pcg64(PcgDev D)
         beta = rzn / rz;
         rz = rzn;
         double* tmp = pp; pp = pc; pc = tmp;
+    }
+    if (it > D.max_iter) it = D.max_iter;
+    cg_finish(D, it, conv, init, fin, rel, mx);
+    if (!conv && b == 0 && threadIdx.x == 0) set_status(D.status, 2, ST_PCG, it, R_PCG_MAXIT);
+}
+
+// ------------------------------------------- register-resident FP64 PCG
+// Same algorithm as k_pcg64, for meshes where every thread owns at most RMAX
+// rows (slices s_beg + warp + 8r, lane = row within the slice).  The row
+// state -- residual, search direction, q, diagonal and flags -- stays in
+// registers for the whole solve; each iteration writes the new direction
+// (double-buffered, for the neighbours' on-the-fly update), z and the
+// pressure to global memory.  Each row's pair entries are fetched eight at a time before
+// the neighbour gathers are issued, so a lane keeps many loads in flight.
+template <int RMAX>
+__global__ void __launch_bounds__(PCG_THREADS, 2) k_pcg64r(PcgDev D)
+{
+    const int G = gridDim.x, b = blockIdx.x;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int s_beg = (int)((long long)b * D.nslices / G);
+    const int s_end = (int)((long long)(b + 1) * D.nslices / G);
+    int phase = 0;
+    const int N = D.N;
+
+    double r[RMAX], p[RMAX], q[RMAX], dg[RMAX];
+    bool fr[RMAX];
+    int row[RMAX];
+#pragma unroll
+    for (int k = 0; k < RMAX; ++k) {
+        const int s = s_beg + warp + PCG_WARPS * k;
+        row[k] = (s < s_end) ? s * 32 + lane : -1;
+        if (row[k] >= N) row[k] = -1;
+        r[k] = p[k] = q[k] = dg[k] = 0.0;
+        fr[k] = false;
+    }
+
+    // off[k] = sum_j A_ij v_j over row k's pair entries, v_j = beta*pp_j + zz_j
+    // (v = zz when pp is null).  All of the thread's rows advance chunk by
+    // chunk together, so RMAX*CH coefficient loads and then RMAX*CH gathers
+    // are in flight at once; each row still accumulates in ascending k.
+    constexpr int CH = (RMAX >= 8) ? 1 : (RMAX >= 4) ? 2 : 8;
+    long long base[RMAX];
+    int wr[RMAX];
+    int wmax = 0;
+#pragma unroll
+    for (int k = 0; k < RMAX; ++k) {
+        base[k] = 0;
+        wr[k] = 0;
+        if (row[k] >= 0) {
+            const int s = row[k] >> 5;
+            base[k] = D.slice_off[s] + lane;
+            wr[k] = D.slice_w[s];
+            wmax = wr[k] > wmax ? wr[k] : wmax;
+        }
+    }
+    auto offdiag_all = [&](double beta, const double* pp, const double* zz, double* off) {
+#pragma unroll
+        for (int k = 0; k < RMAX; ++k) off[k] = 0.0;
+        for (int k0 = 0; k0 < wmax; k0 += CH) {
+            int c[RMAX][CH];
+            double v[RMAX][CH], g[RMAX][CH];
+#pragma unroll
+            for (int k = 0; k < RMAX; ++k)
+#pragma unroll
+                for (int u = 0; u < CH; ++u) {
+                    const bool ok = k0 + u < wr[k];
+                    c[k][u] = ok ? D.col[base[k] + 32LL * (k0 + u)] : 0;
+                    v[k][u] = ok ? D.val[base[k] + 32LL * (k0 + u)] : 0.0;
+                }
+#pragma unroll
+            for (int k = 0; k < RMAX; ++k)
+#pragma unroll
+                for (int u = 0; u < CH; ++u) {
+                    const bool ok = k0 + u < wr[k];
+                    g[k][u] = ok ? (pp ? fma(beta, __ldcg(pp + c[k][u]), __ldcg(zz + c[k][u])) : __ldcg(zz + c[k][u])) : 0.0;
+                }
+#pragma unroll
+            for (int k = 0; k < RMAX; ++k)
+#pragma unroll
+                for (int u = 0; u < CH; ++u) off[k] = fma(v[k][u], g[k][u], off[k]);
+        }
+    };
+
+    // ---- r0 = b - A p0, z0; direction buffer 0 cleared for iteration 1
+    Acc4 acc{0.0, 0.0, 0.0, 0.0};
+    double off[RMAX];
+    offdiag_all(0.0, nullptr, D.pres, off);
+#pragma unroll
+    for (int k = 0; k < RMAX; ++k) {
+        const int i = row[k];
+        if (i < 0) continue;
+        const uint8_t f = D.nflag[i];
+        const bool active = f & 1;
+        fr[k] = (f & 1) && !(f & 4);
+        dg[k] = D.pdiag[i];
+        const double y = fma(dg[k], D.pres[i], off[k]);
+        double ri = active ? D.rhs1[i] - y : 0.0;
+        if (!fr[k]) ri = 0.0;
+        double zi = 0.0;
+        if (fr[k]) {
+            if (D.precond) {
+                if (!(isfinite(dg[k]) && dg[k] > 1.0e-30)) acc.flag = fmax(acc.flag, 1.0);
+                else zi = ri / dg[k];
+            } else {
+                zi = ri;
+            }
+            if (!isfinite(ri)) acc.flag = fmax(acc.flag, 2.0);
+            acc.a = fma(ri, ri, acc.a);
+            acc.b = fma(ri, zi, acc.b);
+            acc.mx = fmax(acc.mx, fabs(ri));
+        }
+        r[k] = ri;
+        D.z[i] = zi;
+        D.pA[i] = 0.0;
+    }
+    Acc4 t = Acc4{0.0, 0.0, 0.0, 0.0};
+    if (!grid_allreduce(acc, D, phase, t)) return;
+    ++phase;
+    const double init = sqrt(t.a);
+    if (init <= 1.0e-300) { cg_finish(D, 0, 1, init, init, 0.0, t.mx); return; }
+    if (cg_converged(D.conv_test, 1.0, t.mx, D.rel_tol, D.abs_tol)) { cg_finish(D, 0, 1, init, init, 1.0, t.mx); return; }
+    if (t.flag >= 2.0) { if (b == 0 && threadIdx.x == 0) set_status(D.status, 4, ST_PCG, 0, R_PCG_RESID); return; }
+    if (t.flag >= 1.0) { if (b == 0 && threadIdx.x == 0) set_status(D.status, 1, ST_PCG, 0, R_PCG_DIAG); return; }
+    double rz = t.b;
+    if (rz <= 1.0e-300 || !isfinite(rz)) { if (b == 0 && threadIdx.x == 0) set_status(D.status, 3, ST_PCG, 0, R_PCG_RZ0); return; }
+
+    double beta = 0.0, fin = init, rel = 1.0, mx = t.mx;
+    int it = 0, conv = 0;
+    for (it = 1; it <= D.max_iter; ++it) {
+        const double* pprev = (it & 1) ? D.pA : D.pB;
+        double* pnew = (it & 1) ? D.pB : D.pA;
+        // ---- p = z + beta p (own rows), q = A p with neighbours' p formed on the fly
+        Acc4 pa{0.0, 0.0, 0.0, 0.0};
+        offdiag_all(beta, pprev, D.z, off);
+#pragma unroll
+        for (int k = 0; k < RMAX; ++k) {
+            const int i = row[k];
+            if (i < 0) continue;
+            p[k] = fr[k] ? fma(beta, p[k], D.z[i]) : 0.0;
+            pnew[i] = p[k];
+            q[k] = fr[k] ? fma(dg[k], p[k], off[k]) : 0.0;
+            if (fr[k]) pa.a = fma(p[k], q[k], pa.a);
+        }
+        t = Acc4{0.0, 0.0, 0.0, 0.0};
+        if (!grid_allreduce(pa, D, phase, t)) return;
+        ++phase;
+        const double pAp = t.a;
+        if (fabs(pAp) <= 1.0e-300 || !isfinite(pAp)) { if (b == 0 && threadIdx.x == 0) set_status(D.status, 3, ST_PCG, it, R_PCG_PAP); return; }
+        const double alpha = rz / pAp;
+
+        // ---- x += alpha p, r -= alpha q, z = M^-1 r
+        Acc4 rr{0.0, 0.0, 0.0, 0.0};
+#pragma unroll
+        for (int k = 0; k < RMAX; ++k) {
+            const int i = row[k];
+            if (i < 0 || !fr[k]) continue;
+            D.pres[i] = fma(alpha, p[k], D.pres[i]);
+            r[k] = fma(-alpha, q[k], r[k]);
+            const double zk = D.precond ? r[k] / dg[k] : r[k];
+            D.z[i] = zk;
+            if (!isfinite(r[k])) rr.flag = 1.0;
+            rr.a = fma(r[k], r[k], rr.a);
+            rr.b = fma(r[k], zk, rr.b);
+            rr.mx = fmax(rr.mx, fabs(r[k]));
+        }
+        t = Acc4{0.0, 0.0, 0.0, 0.0};
+        if (!grid_allreduce(rr, D, phase, t)) return;
+        ++phase;
+        fin = sqrt(t.a);
+        mx = t.mx;
+        rel = fin / init;
+        if (cg_converged(D.conv_test, rel, mx, D.rel_tol, D.abs_tol)) { conv = 1; break; }
+        if (t.flag > 0.0) { if (b == 0 && threadIdx.x == 0) set_status(D.status, 4, ST_PCG, it, R_PCG_RESID); return; }
+        const double rzn = t.b;
+        if (rzn <= 1.0e-300 || !isfinite(rzn)) { if (b == 0 && threadIdx.x == 0) set_status(D.status, 3, ST_PCG, it, R_PCG_RZ); return; }
+        beta = rzn / rz;
+        rz = rzn;
+    }
+    if (it > D.max_iter) it = D.max_iter;
+    cg_finish(D, it, conv, init, fin, rel, mx);
+    if (!conv && b == 0 && threadIdx.x == 0) set_status(D.status, 2, ST_PCG, it, R_PCG_MAXIT);
+}
+
+// ---------------------------------------- halo-staged FP64 PCG (default)
+// The register-resident algorithm of k_pcg64r with the neighbour gathers
+// served from shared memory.  Each persistent CTA owns a contiguous block of
+// slices; the host lists, per CTA, the distinct nodes its rows reference (its
+// halo, own rows included) and rewrites every pair entry's column as a 16-bit
+// index into that list.  Each phase the CTA stages the values it needs
+// (v = beta*p_prev + z, or the pressure in phase 0) for its halo into shared
+// memory with one cooperative, mostly contiguous load, and the matvec then
+// reads only the streamed coefficients from global memory.  The local column
+// indices stay in shared memory for the whole solve.
+template <int RMAX>
+__global__ void __launch_bounds__(PCG_THREADS, 2) k_pcg64h(PcgDev D)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int G = gridDim.x, b = blockIdx.x;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int s_beg = (int)((long long)b * D.nslices / G);
+    const int s_end = (int)((long long)(b + 1) * D.nslices / G);
+    const long long S0 = D.slice_off[s_beg];
+    const int nsl = (int)(D.slice_off[s_end] - S0);
+    const int h0 = D.halo_ptr[b];
+    const int nh = D.halo_ptr[b + 1] - h0;
+    double* vh = reinterpret_cast<double*>(smem_raw);
+    int* hidx = reinterpret_cast<int*>(vh + D.halo_max);
+    unsigned short* lcs = reinterpret_cast<unsigned short*>(hidx + D.halo_max);
+    for (int k = threadIdx.x; k < nh; k += PCG_THREADS) hidx[k] = D.halo_idx[h0 + k];
+    for (int k = threadIdx.x; k < nsl; k += PCG_THREADS) lcs[k] = D.lcol[S0 + k];
+    int phase = 0;
+    const int N = D.N;
+
+    double r[RMAX], p[RMAX], q[RMAX], dg[RMAX];
+    bool fr[RMAX];
+    int row[RMAX], lbase[RMAX], wr[RMAX];
+    int wmax = 0;
+#pragma unroll
+    for (int k = 0; k < RMAX; ++k) {
+        const int s = s_beg + warp + PCG_WARPS * k;
+        row[k] = (s < s_end) ? s * 32 + lane : -1;
+        lbase[k] = 0;
+        wr[k] = 0;
+        if (s < s_end) {
+            lbase[k] = (int)(D.slice_off[s] - S0) + lane;
+            wr[k] = D.slice_w[s];
+            wmax = wr[k] > wmax ? wr[k] : wmax;
+        }
+        if (row[k] >= N) row[k] = -1;
+        r[k] = p[k] = q[k] = dg[k] = 0.0;
+        fr[k] = false;
+    }
+
+    // stage v_j = beta*pp_j + zz_j (v = zz when pp is null) for the halo
+    auto stage = [&](double beta, const double* pp, const double* zz) {
+        __syncthreads();
+        for (int k = threadIdx.x; k < nh; k += PCG_THREADS) {
+            const int j = hidx[k];
+            vh[k] = pp ? fma(beta, __ldcg(pp + j), __ldcg(zz + j)) : __ldcg(zz + j);
+        }
+        __syncthreads();
+    };
+    constexpr int CH = (RMAX >= 8) ? 2 : (RMAX >= 4) ? 4 : 8;
+    auto offdiag_all = [&](double* off) {
+#pragma unroll
+        for (int k = 0; k < RMAX; ++k) off[k] = 0.0;
+        for (int k0 = 0; k0 < wmax; k0 += CH) {
+            double v[RMAX][CH];
+#pragma unroll
+            for (int k = 0; k < RMAX; ++k)
+#pragma unroll
+                for (int u = 0; u < CH; ++u)
+                    v[k][u] = (k0 + u < wr[k]) ? __ldcg(D.val + S0 + lbase[k] + 32 * (k0 + u)) : 0.0;
+#pragma unroll
+            for (int k = 0; k < RMAX; ++k)
+#pragma unroll
+                for (int u = 0; u < CH; ++u) {
+                    const double g = (k0 + u < wr[k]) ? vh[lcs[lbase[k] + 32 * (k0 + u)]] : 0.0;
+                    off[k] = fma(v[k][u], g, off[k]);
+                }
+        }
+    };
+
+    // ---- r0 = b - A p0, z0; direction buffer 0 cleared for iteration 1
+    Acc4 acc{0.0, 0.0, 0.0, 0.0};
+    double off[RMAX];
+    stage(0.0, nullptr, D.pres);
+    offdiag_all(off);
+#pragma unroll
+    for (int k = 0; k < RMAX; ++k) {
+        const int i = row[k];
+        if (i < 0) continue;
+        const uint8_t f = D.nflag[i];
+        const bool active = f & 1;
+        fr[k] = (f & 1) && !(f & 4);
+        dg[k] = D.pdiag[i];
+        const double y = fma(dg[k], D.pres[i], off[k]);
+        double ri = active ? D.rhs1[i] - y : 0.0;
+        if (!fr[k]) ri = 0.0;
+        double zi = 0.0;
+        if (fr[k]) {
+            if (D.precond) {
+                if (!(isfinite(dg[k]) && dg[k] > 1.0e-30)) acc.flag = fmax(acc.flag, 1.0);
+                else zi = ri / dg[k];
+            } else {
+                zi = ri;
+            }
+            if (!isfinite(ri)) acc.flag = fmax(acc.flag, 2.0);
+            acc.a = fma(ri, ri, acc.a);
+            acc.b = fma(ri, zi, acc.b);
+            acc.mx = fmax(acc.mx, fabs(ri));
+        }
+        r[k] = ri;
+        D.z[i] = zi;
+        D.pA[i] = 0.0;
+    }
+    Acc4 t = Acc4{0.0, 0.0, 0.0, 0.0};
+    if (!grid_allreduce(acc, D, phase, t)) return;
+    ++phase;
+    const double init = sqrt(t.a);
+    if (init <= 1.0e-300) { cg_finish(D, 0, 1, init, init, 0.0, t.mx); return; }
+    if (cg_converged(D.conv_test, 1.0, t.mx, D.rel_tol, D.abs_tol)) { cg_finish(D, 0, 1, init, init, 1.0, t.mx); return; }
+    if (t.flag >= 2.0) { if (b == 0 && threadIdx.x == 0) set_status(D.status, 4, ST_PCG, 0, R_PCG_RESID); return; }
+    if (t.flag >= 1.0) { if (b == 0 && threadIdx.x == 0) set_status(D.status, 1, ST_PCG, 0, R_PCG_DIAG); return; }
+    double rz = t.b;
+    if (rz <= 1.0e-300 || !isfinite(rz)) { if (b == 0 && threadIdx.x == 0) set_status(D.status, 3, ST_PCG, 0, R_PCG_RZ0); return; }
+
+    double beta = 0.0, fin = init, rel = 1.0, mx = t.mx;
+    int it = 0, conv = 0;
+    for (it = 1; it <= D.max_iter; ++it) {
+        const double* pprev = (it & 1) ? D.pA : D.pB;
+        double* pnew = (it & 1) ? D.pB : D.pA;
+        Acc4 pa{0.0, 0.0, 0.0, 0.0};
+        stage(beta, pprev, D.z);
+        offdiag_all(off);
+#pragma unroll
+        for (int k = 0; k < RMAX; ++k) {
+            const int i = row[k];
+            if (i < 0) continue;
+            p[k] = fr[k] ? fma(beta, p[k], D.z[i]) : 0.0;
+            pnew[i] = p[k];
+            q[k] = fr[k] ? fma(dg[k], p[k], off[k]) : 0.0;
+            if (fr[k]) pa.a = fma(p[k], q[k], pa.a);
+        }
+        t = Acc4{0.0, 0.0, 0.0, 0.0};
+        if (!grid_allreduce(pa, D, phase, t)) return;
+        ++phase;
+        const double pAp = t.a;
+        if (fabs(pAp) <= 1.0e-300 || !isfinite(pAp)) { if (b == 0 && threadIdx.x == 0) set_status(D.status, 3, ST_PCG, it, R_PCG_PAP); return; }
+        const double alpha = rz / pAp;
+
+        Acc4 rr{0.0, 0.0, 0.0, 0.0};
+#pragma unroll
+        for (int k = 0; k < RMAX; ++k) {
+            const int i = row[k];
+            if (i < 0 || !fr[k]) continue;
+            D.pres[i] = fma(alpha, p[k], D.pres[i]);
+            r[k] = fma(-alpha, q[k], r[k]);
+            const double zk = D.precond ? r[k] / dg[k] : r[k];
+            D.z[i] = zk;
+            if (!isfinite(r[k])) rr.flag = 1.0;
+            rr.a = fma(r[k], r[k], rr.a);
+            rr.b = fma(r[k], zk, rr.b);
+            rr.mx = fmax(rr.mx, fabs(r[k]));
+        }
+        t = Acc4{0.0, 0.0, 0.0, 0.0};
+        if (!grid_allreduce(rr, D, phase, t)) return;
+        ++phase;
+        fin = sqrt(t.a);
+        mx = t.mx;
+        rel = fin / init;
+        if (cg_converged(D.conv_test, rel, mx, D.rel_tol, D.abs_tol)) { conv = 1; break; }
+        if (t.flag > 0.0) { if (b == 0 && threadIdx.x == 0) set_status(D.status, 4, ST_PCG, it, R_PCG_RESID); return; }
+        const double rzn = t.b;
+        if (rzn <= 1.0e-300 || !isfinite(rzn)) { if (b == 0 && threadIdx.x == 0) set_status(D.status, 3, ST_PCG, it, R_PCG_RZ); return; }
+        beta = rzn / rz;
+        rz = rzn;
     }
     if (it > D.max_iter) it = D.max_iter;
     cg_finish(D, it, conv, init, fin, rel, mx);
@@ -336,7 +725,7 @@ cbs3d_status selftest_wait_timeout(int device, int* observed)
 
 // ============================================================ PcgEngine
 void PcgEngine::init(const HostModel& m, const uint8_t* nflag, const double* pfix, DevStatus* status,
-                     int device, int blocks_override, bool mixed_mode)
+                     int device, int blocks_override, bool mixed_mode, int kernel_choice)
 {
     N = m.N;
     E = m.E;
@@ -372,15 +761,85 @@ void PcgEngine::init(const HostModel& m, const uint8_t* nflag, const double* pfi
     d_pfix = pfix;
     d_status = status;
 
-    int sms = 0, per_sm = 0;
+    int sms = 0;
     CUDA_OK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
-    CUDA_OK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_pcg64, PCG_THREADS, 0));
-    int g = sms * (per_sm < 2 ? per_sm : 2);
-    if (blocks_override > 0 && blocks_override < g) g = blocks_override;
-    // never more CTAs than slices
-    if (g > nslices) g = nslices > 0 ? nslices : 1;
-    nblocks = g;
-    d_part = dalloc<double>(static_cast<size_t>(2 * nblocks * 8));
+    // Register-resident kernel when every thread's rows fit its register
+    // arrays; otherwise the kernel that keeps the vectors in global memory.
+    auto grid_for = [&](const void* fn) {
+        int per_sm = 0;
+        CUDA_OK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, PCG_THREADS, 0));
+        int g = sms * (per_sm < 2 ? per_sm : 2);
+        if (blocks_override > 0 && blocks_override < g) g = blocks_override;
+        if (g > nslices) g = nslices > 0 ? nslices : 1;
+        return g;
+    };
+    rmax = 0;
+    variant = 1;
+    nblocks = grid_for(reinterpret_cast<const void*>(k_pcg64));
+    const int rm[4] = {1, 2, 4, 8};
+    if (kernel_choice == 0 || kernel_choice == 3) {
+        const void* hc[4] = {reinterpret_cast<const void*>(k_pcg64h<1>), reinterpret_cast<const void*>(k_pcg64h<2>),
+                             reinterpret_cast<const void*>(k_pcg64h<4>), reinterpret_cast<const void*>(k_pcg64h<8>)};
+        for (int c = 0; c < 4 && variant == 1; ++c) {
+            int per_sm = 0;
+            CUDA_OK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, hc[c], PCG_THREADS, 0));
+            int g = sms * (per_sm < 2 ? per_sm : 2);
+            if (blocks_override > 0 && blocks_override < g) g = blocks_override;
+            if (g > nslices) g = nslices > 0 ? nslices : 1;
+            const int per_cta = (nslices + g - 1) / g;
+            if ((per_cta + PCG_WARPS - 1) / PCG_WARPS > rm[c]) continue;
+            // halo of every CTA: distinct columns of its slot range, sorted
+            std::vector<int> hptr(static_cast<size_t>(g) + 1, 0), hidx;
+            std::vector<unsigned short> lcol(static_cast<size_t>(nslots), 0);
+            int hmax = 0;
+            long long smax = 0;
+            bool fits = true;
+            std::vector<int> cols;
+            for (int bb = 0; bb < g && fits; ++bb) {
+                const int sb = static_cast<int>(static_cast<long long>(bb) * nslices / g);
+                const int se = static_cast<int>(static_cast<long long>(bb + 1) * nslices / g);
+                const long long a0 = P.slice_off[static_cast<size_t>(sb)], a1 = P.slice_off[static_cast<size_t>(se)];
+                cols.assign(P.col.begin() + a0, P.col.begin() + a1);
+                std::sort(cols.begin(), cols.end());
+                cols.erase(std::unique(cols.begin(), cols.end()), cols.end());
+                if (cols.size() > 65535) { fits = false; break; }
+                for (long long t = a0; t < a1; ++t)
+                    lcol[static_cast<size_t>(t)] = static_cast<unsigned short>(
+                        std::lower_bound(cols.begin(), cols.end(), P.col[static_cast<size_t>(t)]) - cols.begin());
+                hidx.insert(hidx.end(), cols.begin(), cols.end());
+                hptr[static_cast<size_t>(bb) + 1] = static_cast<int>(hidx.size());
+                hmax = std::max(hmax, static_cast<int>(cols.size()));
+                smax = std::max(smax, a1 - a0);
+            }
+            if (!fits) continue;
+            const size_t smem = static_cast<size_t>(hmax) * 12 + static_cast<size_t>(smax) * 2 + 16;
+            if (smem > 200 * 1024) continue;
+            CUDA_OK(cudaFuncSetAttribute(hc[c], cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
+            CUDA_OK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, hc[c], PCG_THREADS, smem));
+            if (per_sm * sms < g) continue;
+            variant = 3;
+            rmax = rm[c];
+            nblocks = g;
+            halo_smem = smem;
+            d_halo_ptr = dalloc<int>(hptr.size());
+            d_halo_idx = dalloc<int>(hidx.size());
+            d_lcol = dalloc<unsigned short>(lcol.size());
+            CUDA_OK(cudaMemcpy(d_halo_ptr, hptr.data(), hptr.size() * sizeof(int), cudaMemcpyHostToDevice));
+            CUDA_OK(cudaMemcpy(d_halo_idx, hidx.data(), hidx.size() * sizeof(int), cudaMemcpyHostToDevice));
+            if (!lcol.empty()) CUDA_OK(cudaMemcpy(d_lcol, lcol.data(), lcol.size() * sizeof(unsigned short), cudaMemcpyHostToDevice));
+            dev_halo_max = hmax;
+        }
+    }
+    if (variant == 1 && kernel_choice != 1) {
+        const void* cands[4] = {reinterpret_cast<const void*>(k_pcg64r<1>), reinterpret_cast<const void*>(k_pcg64r<2>),
+                                reinterpret_cast<const void*>(k_pcg64r<4>), reinterpret_cast<const void*>(k_pcg64r<8>)};
+        for (int c = 0; c < 4; ++c) {
+            const int g = grid_for(cands[c]);
+            const int per_cta = (nslices + g - 1) / g;
+            if ((per_cta + PCG_WARPS - 1) / PCG_WARPS <= rm[c]) { rmax = rm[c]; nblocks = g; variant = 2; break; }
+        }
+    }
+    d_part = dalloc<double>(static_cast<size_t>(nblocks) * 4 + 8);
     d_bar = dalloc<unsigned>(4);
     d_out = dalloc<CgOut>(1);
     CUDA_OK(cudaMemset(d_bar, 0, 4 * sizeof(unsigned)));
@@ -396,16 +855,18 @@ void PcgEngine::init(const HostModel& m, const uint8_t* nflag, const double* pfi
         dev.q32 = d_f32 + 4 * n; dev.x32 = d_f32 + 5 * n; dev.dinv32 = d_f32 + 6 * n;
     }
     dev.part = d_part; dev.bar = d_bar; dev.status = d_status; dev.out = d_out;
+    dev.halo_ptr = d_halo_ptr; dev.halo_idx = d_halo_idx; dev.lcol = d_lcol; dev.halo_max = dev_halo_max;
 }
 
 void PcgEngine::release()
 {
     void* ptrs[] = {d_slice_off, d_slice_w, d_col, d_cptr, d_cent, d_val, d_val32, d_r, d_z, d_pA,
-                    d_pB, d_q, d_f32, d_part, d_bar, d_out};
+                    d_pB, d_q, d_f32, d_part, d_bar, d_out, d_halo_ptr, d_halo_idx, d_lcol};
     for (void* p : ptrs) if (p) cudaFree(p);
     d_slice_off = nullptr; d_slice_w = nullptr; d_col = nullptr; d_cptr = nullptr; d_cent = nullptr;
     d_val = nullptr; d_val32 = nullptr; d_r = d_z = d_pA = d_pB = d_q = nullptr; d_f32 = nullptr;
     d_part = nullptr; d_bar = nullptr; d_out = nullptr;
+    d_halo_ptr = nullptr; d_halo_idx = nullptr; d_lcol = nullptr;
 }
 
 void PcgEngine::assemble_from_state(const DevState& S, cudaStream_t st)
@@ -440,8 +901,22 @@ cbs3d_status PcgEngine::solve(double* pres, double* rhs1, double* pdiag, int pre
     k_impose<<<(N + 255) / 256, 256, 0, st>>>(D);
     CUDA_OK(cudaMemsetAsync(d_bar, 0, 2 * sizeof(unsigned), st));
     void* args[] = {&D};
+    const void* fn = reinterpret_cast<const void*>(k_pcg64);
+    size_t smem = 0;
+    if (variant == 2) {
+        if (rmax == 1) fn = reinterpret_cast<const void*>(k_pcg64r<1>);
+        else if (rmax == 2) fn = reinterpret_cast<const void*>(k_pcg64r<2>);
+        else if (rmax == 4) fn = reinterpret_cast<const void*>(k_pcg64r<4>);
+        else fn = reinterpret_cast<const void*>(k_pcg64r<8>);
+    } else if (variant == 3) {
+        if (rmax == 1) fn = reinterpret_cast<const void*>(k_pcg64h<1>);
+        else if (rmax == 2) fn = reinterpret_cast<const void*>(k_pcg64h<2>);
+        else if (rmax == 4) fn = reinterpret_cast<const void*>(k_pcg64h<4>);
+        else fn = reinterpret_cast<const void*>(k_pcg64h<8>);
+        smem = halo_smem;
+    }
     if (ev0) CUDA_OK(cudaEventRecord(ev0, st));
-    CUDA_OK(cudaLaunchCooperativeKernel(reinterpret_cast<void*>(k_pcg64), dim3(nblocks), dim3(PCG_THREADS), args, 0, st));
+    CUDA_OK(cudaLaunchCooperativeKernel(fn, dim3(nblocks), dim3(PCG_THREADS), args, smem, st));
     if (ev1) CUDA_OK(cudaEventRecord(ev1, st));
     if (sync) CUDA_OK(cudaStreamSynchronize(st));
     return CBS3D_OK;
@@ -466,6 +941,19 @@ cbs3d_status PcgEngine::read_result(cbs3d_cg_result& r, cudaStream_t st)
 
 size_t PcgEngine::bytes_per_iter() const
 {
+    if (variant == 3) {
+        // coefficient per pair entry; per node: halo staging of z and the
+        // previous direction (each node is in about one CTA's halo per owner
+        // plus the overlap, counted once here), z read back, new direction and
+        // z written, pressure read and written
+        return static_cast<size_t>(nnz_offdiag) * 8 + static_cast<size_t>(N) * 56;
+    }
+    if (rmax > 0) {
+        // coefficient + column per pair entry; per node the z and previous
+        // direction gathered once, z read back, new direction and z written,
+        // pressure read and written
+        return static_cast<size_t>(nnz_offdiag) * 12 + static_cast<size_t>(N) * 56;
+    }
     // Phase A: coefficient + column per pair entry; z and previous p of the
     // row (16 B), pdiag (8), new p written (8), q written (8), node flag (1).
     // Phase B: q, r, pres, pdiag read (32), r, pres, z written (24).

@@ -36,7 +36,11 @@ struct PcgDev {
     double *pres, *rhs1, *pdiag;
     double *r, *z, *pA, *pB, *q;
     float *r32, *z32, *pA32, *pB32, *q32, *x32, *dinv32;
-    double* part;                // nblocks * 8
+    const int* halo_ptr;         // nblocks+1: each CTA's halo node list in halo_idx
+    const int* halo_idx;
+    const unsigned short* lcol;  // per slot: column as an index into its CTA's halo
+    int halo_max;                // largest halo (shared-memory sizing)
+    double* part;                // nblocks * 4 partials + 8 totals
     unsigned* bar;               // [0] count, [1] generation
     DevStatus* status;
     CgOut* out;
@@ -45,8 +49,10 @@ struct PcgDev {
 // Owns the device copies of the pattern and the PCG work vectors.
 class PcgEngine {
 public:
+    // kernel_choice: 0 automatic, 1 vectors in global memory, 2 register-resident rows,
+    // 3 register-resident rows with the halo staged in shared memory
     void init(const HostModel& m, const uint8_t* d_nflag, const double* d_pfix, DevStatus* d_status,
-              int device, int blocks_override, bool mixed);
+              int device, int blocks_override, bool mixed, int kernel_choice = 0);
     void release();
     // ELL values from gstifE*delte (step path) or from a caller's gstif[6E].
     void assemble_from_state(const DevState& S, cudaStream_t st);
@@ -62,6 +68,12 @@ public:
     void multiply(const double* d_pdiag, const double* d_x, double* d_y, cudaStream_t st);
 
     bool mixed = false;
+    int rmax = 0;            // rows per thread of the register-resident kernels (0: global kernel)
+    int variant = 1;         // 1 global vectors, 2 register rows, 3 register rows + shared-memory halo
+    size_t halo_smem = 0;    // dynamic shared memory of the halo kernel
+    int *d_halo_ptr = nullptr, *d_halo_idx = nullptr;
+    unsigned short* d_lcol = nullptr;
+    int dev_halo_max = 0;
     double inner_tol = 1.0e-5;
     int N = 0, E = 0, nslices = 0, nblocks = 0;
     long long nslots = 0, ncontrib = 0;
