@@ -695,6 +695,347 @@ __global__ void __launch_bounds__(PCG_THREADS, 2) k_pcg64h(PcgDev D)
     if (!conv && b == 0 && threadIdx.x == 0) set_status(D.status, 2, ST_PCG, it, R_PCG_MAXIT);
 }
 
+// --------------------------- single-synchronisation halo PCG (default)
+// Chronopoulos-Gear form of the same Jacobi-PCG: the matvec is applied to z
+// (w = A z) and the direction's product s = A p follows the recurrence
+// s = w + beta*s, so alpha and beta come from one grid reduction of
+// (r.z, z.w, r.r, max|r|) per iteration instead of two.  Residuals, stopping
+// test, iteration count and breakdown checks keep the reference's meaning
+// (src/linalg/ConjugateGradient.cpp:725-853); in exact arithmetic the iterates
+// equal the standard PCG's.  Neighbour values of the new z are formed while
+// the halo is staged, from the previous iteration's r, w, s (double-buffered
+// by iteration parity) and the diagonal, with the same operations the owner
+// applies to its own rows.
+struct Acc6 {
+    double a, b, c, mx, flag;
+};
+
+__device__ __forceinline__ bool grid_allreduce3(Acc6 v, const PcgDev& D, int phase, Acc6& out)
+{
+    __shared__ double sm[PCG_WARPS][5];
+    __shared__ double tot[5];
+    __shared__ int s_last, s_ok;
+    const int G = gridDim.x;
+    for (int o = 16; o > 0; o >>= 1) {
+        v.a += __shfl_down_sync(0xffffffffu, v.a, o);
+        v.b += __shfl_down_sync(0xffffffffu, v.b, o);
+        v.c += __shfl_down_sync(0xffffffffu, v.c, o);
+        v.mx = fmax(v.mx, __shfl_down_sync(0xffffffffu, v.mx, o));
+        v.flag = fmax(v.flag, __shfl_down_sync(0xffffffffu, v.flag, o));
+    }
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    if (lane == 0) { sm[w][0] = v.a; sm[w][1] = v.b; sm[w][2] = v.c; sm[w][3] = v.mx; sm[w][4] = v.flag; }
+    __syncthreads();
+    unsigned* cnt = D.bar;
+    unsigned* gen = D.bar + 1;
+    double* totals = D.part + (size_t)G * 8 + (size_t)(phase & 1) * 8;
+    if (threadIdx.x == 0) {
+        double t[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
+        for (int k = 0; k < PCG_WARPS; ++k) {
+            t[0] += sm[k][0]; t[1] += sm[k][1]; t[2] += sm[k][2];
+            t[3] = fmax(t[3], sm[k][3]); t[4] = fmax(t[4], sm[k][4]);
+        }
+        double* p = D.part + (size_t)blockIdx.x * 8;
+        for (int k = 0; k < 5; ++k) __stcg(p + k, t[k]);
+        const unsigned g = ld_acquire(gen);
+        unsigned arrived;
+        asm volatile("atom.add.acq_rel.gpu.global.u32 %0, [%1], 1;" : "=r"(arrived) : "l"(cnt) : "memory");
+        s_last = (arrived == (unsigned)G - 1) ? 1 : 0;
+        s_ok = 1;
+        if (!s_last) {
+            const long long t0 = clock64();
+            while (ld_acquire(gen) == g) {
+                if (ld_relaxed_int(&D.status->code) != 0) { s_ok = 0; break; }
+                if (clock64() - t0 > (1LL << 31)) {
+                    set_status(D.status, 5 /*CBS3D_TIMEOUT*/, ST_PCG, 0, R_PCG_BARRIER);
+                    s_ok = 0;
+                    break;
+                }
+                __nanosleep(20);
+            }
+            if (s_ok) for (int k = 0; k < 5; ++k) tot[k] = __ldcg(totals + k);
+        }
+    }
+    __syncthreads();
+    if (s_last) {
+        double t[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
+        for (int k = threadIdx.x; k < G; k += PCG_THREADS) {
+            const double* p = D.part + (size_t)k * 8;
+            t[0] += __ldcg(p); t[1] += __ldcg(p + 1); t[2] += __ldcg(p + 2);
+            t[3] = fmax(t[3], __ldcg(p + 3)); t[4] = fmax(t[4], __ldcg(p + 4));
+        }
+        for (int o = 16; o > 0; o >>= 1) {
+            t[0] += __shfl_down_sync(0xffffffffu, t[0], o);
+            t[1] += __shfl_down_sync(0xffffffffu, t[1], o);
+            t[2] += __shfl_down_sync(0xffffffffu, t[2], o);
+            t[3] = fmax(t[3], __shfl_down_sync(0xffffffffu, t[3], o));
+            t[4] = fmax(t[4], __shfl_down_sync(0xffffffffu, t[4], o));
+        }
+        __syncthreads();
+        if (lane == 0) for (int k = 0; k < 5; ++k) sm[w][k] = t[k];
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            double u[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
+            for (int k = 0; k < PCG_WARPS; ++k) {
+                u[0] += sm[k][0]; u[1] += sm[k][1]; u[2] += sm[k][2];
+                u[3] = fmax(u[3], sm[k][3]); u[4] = fmax(u[4], sm[k][4]);
+            }
+            for (int k = 0; k < 5; ++k) { tot[k] = u[k]; __stcg(totals + k, u[k]); }
+            atomicExch(cnt, 0u);
+            asm volatile("red.release.gpu.global.add.u32 [%0], 1;" :: "l"(gen) : "memory");
+            if (ld_relaxed_int(&D.status->code) != 0) s_ok = 0;
+        }
+    }
+    __syncthreads();
+    out = Acc6{tot[0], tot[1], tot[2], tot[3], tot[4]};
+    const bool ok = s_ok != 0;
+    __syncthreads();
+    return ok;
+}
+
+template <int RMAX>
+__global__ void __launch_bounds__(PCG_THREADS, 2) k_pcg64c(PcgDev D)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int G = gridDim.x, b = blockIdx.x;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int s_beg = (int)((long long)b * D.nslices / G);
+    const int s_end = (int)((long long)(b + 1) * D.nslices / G);
+    const long long S0 = D.slice_off[s_beg];
+    const int nsl = (int)(D.slice_off[s_end] - S0);
+    const int h0 = D.halo_ptr[b];
+    const int nh = D.halo_ptr[b + 1] - h0;
+    double* vh = reinterpret_cast<double*>(smem_raw);
+    double* dzh = vh + D.halo_max;
+    int* hidx = reinterpret_cast<int*>(dzh + D.halo_max);
+    unsigned short* lcs = reinterpret_cast<unsigned short*>(hidx + D.halo_max);
+    for (int k = threadIdx.x; k < nh; k += PCG_THREADS) hidx[k] = D.halo_idx[h0 + k];
+    for (int k = threadIdx.x; k < nsl; k += PCG_THREADS) lcs[k] = D.lcol[S0 + k];
+    int phase = 0;
+    const int N = D.N;
+    // parity buffers: r in r/pA, w in q/pB, s in z/dz(+N)... laid out by the engine
+    double* rb[2] = {D.r, D.r + N};
+    double* wb[2] = {D.q, D.q + N};
+    double* sb[2] = {D.pA, D.pB};
+    double* dz = D.z;   // free ? diagonal : +inf  (z = r / dz)
+
+    double r[RMAX], p[RMAX], s[RMAX], w[RMAX], dd[RMAX];
+    bool fr[RMAX];
+    int row[RMAX], lbase[RMAX], wr[RMAX];
+    int wmax = 0;
+#pragma unroll
+    for (int k = 0; k < RMAX; ++k) {
+        const int sl = s_beg + warp + PCG_WARPS * k;
+        row[k] = (sl < s_end) ? sl * 32 + lane : -1;
+        lbase[k] = 0;
+        wr[k] = 0;
+        if (sl < s_end) {
+            lbase[k] = (int)(D.slice_off[sl] - S0) + lane;
+            wr[k] = D.slice_w[sl];
+            wmax = wr[k] > wmax ? wr[k] : wmax;
+        }
+        if (row[k] >= N) row[k] = -1;
+        r[k] = p[k] = s[k] = w[k] = 0.0;
+        dd[k] = __longlong_as_double(0x7ff0000000000000LL);
+        fr[k] = false;
+    }
+    constexpr int CH = (RMAX >= 8) ? 2 : (RMAX >= 4) ? 4 : 8;
+    auto offdiag_all = [&](double* off) {
+#pragma unroll
+        for (int k = 0; k < RMAX; ++k) off[k] = 0.0;
+        for (int k0 = 0; k0 < wmax; k0 += CH) {
+            double v[RMAX][CH];
+#pragma unroll
+            for (int k = 0; k < RMAX; ++k)
+#pragma unroll
+                for (int u = 0; u < CH; ++u)
+                    v[k][u] = (k0 + u < wr[k]) ? __ldcg(D.val + S0 + lbase[k] + 32 * (k0 + u)) : 0.0;
+#pragma unroll
+            for (int k = 0; k < RMAX; ++k)
+#pragma unroll
+                for (int u = 0; u < CH; ++u) {
+                    const double g = (k0 + u < wr[k]) ? vh[lcs[lbase[k] + 32 * (k0 + u)]] : 0.0;
+                    off[k] = fma(v[k][u], g, off[k]);
+                }
+        }
+    };
+
+    // ---- phase 0a: r0 = b - A x0 (constraints as the reference), dz
+    double off[RMAX];
+    __syncthreads();
+    for (int k0 = threadIdx.x; k0 < nh; k0 += 4 * PCG_THREADS) {
+        double a[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            const int k = k0 + u * PCG_THREADS;
+            a[u] = __ldcg(D.pres + (k < nh ? hidx[k] : 0));
+        }
+#pragma unroll
+        for (int u = 0; u < 4; ++u)
+            if (k0 + u * PCG_THREADS < nh) vh[k0 + u * PCG_THREADS] = a[u];
+    }
+    __syncthreads();
+    offdiag_all(off);
+    Acc6 acc{0.0, 0.0, 0.0, 0.0, 0.0};
+#pragma unroll
+    for (int k = 0; k < RMAX; ++k) {
+        const int i = row[k];
+        if (i < 0) continue;
+        const uint8_t f = D.nflag[i];
+        const bool active = f & 1;
+        fr[k] = (f & 1) && !(f & 4);
+        const double pd = D.pdiag[i];
+        const double y = fma(pd, D.pres[i], off[k]);
+        double ri = active ? D.rhs1[i] - y : 0.0;
+        if (!fr[k]) ri = 0.0;
+        if (fr[k]) {
+            if (D.precond) {
+                if (!(isfinite(pd) && pd > 1.0e-30)) acc.flag = fmax(acc.flag, 1.0);
+                dd[k] = pd;
+            } else {
+                dd[k] = 1.0;
+            }
+            if (!isfinite(ri)) acc.flag = fmax(acc.flag, 2.0);
+            acc.c = fma(ri, ri, acc.c);
+            acc.mx = fmax(acc.mx, fabs(ri));
+        }
+        r[k] = ri;
+        rb[0][i] = ri;
+        dz[i] = dd[k];
+        sb[0][i] = 0.0;
+    }
+    Acc6 t{0.0, 0.0, 0.0, 0.0, 0.0};
+    if (!grid_allreduce3(acc, D, phase, t)) return;
+    ++phase;
+    const double init = sqrt(t.c);
+    if (init <= 1.0e-300) { cg_finish(D, 0, 1, init, init, 0.0, t.mx); return; }
+    if (cg_converged(D.conv_test, 1.0, t.mx, D.rel_tol, D.abs_tol)) { cg_finish(D, 0, 1, init, init, 1.0, t.mx); return; }
+    if (t.flag >= 2.0) { if (b == 0 && threadIdx.x == 0) set_status(D.status, 4, ST_PCG, 0, R_PCG_RESID); return; }
+    if (t.flag >= 1.0) { if (b == 0 && threadIdx.x == 0) set_status(D.status, 1, ST_PCG, 0, R_PCG_DIAG); return; }
+
+    // ---- phase 0b: z0 = M^-1 r0, w0 = A z0, gamma0 = (r0,z0), delta0 = (z0,w0)
+    __syncthreads();
+    for (int k0 = threadIdx.x; k0 < nh; k0 += 4 * PCG_THREADS) {
+        double a[4], c[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            const int k = k0 + u * PCG_THREADS;
+            const int j = k < nh ? hidx[k] : 0;
+            a[u] = __ldcg(dz + j);
+            c[u] = __ldcg(rb[0] + j);
+        }
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            const int k = k0 + u * PCG_THREADS;
+            if (k < nh) { dzh[k] = a[u]; vh[k] = c[u] / a[u]; }
+        }
+    }
+    __syncthreads();
+    offdiag_all(off);
+    acc = Acc6{0.0, 0.0, 0.0, 0.0, 0.0};
+#pragma unroll
+    for (int k = 0; k < RMAX; ++k) {
+        const int i = row[k];
+        if (i < 0) continue;
+        const double zi = r[k] / dd[k];
+        w[k] = fr[k] ? fma(D.pdiag[i], zi, off[k]) : 0.0;
+        wb[0][i] = w[k];
+        if (fr[k]) {
+            acc.a = fma(r[k], zi, acc.a);
+            acc.b = fma(zi, w[k], acc.b);
+        }
+    }
+    t = Acc6{0.0, 0.0, 0.0, 0.0, 0.0};
+    if (!grid_allreduce3(acc, D, phase, t)) return;
+    ++phase;
+    double gam = t.a;
+    if (gam <= 1.0e-300 || !isfinite(gam)) { if (b == 0 && threadIdx.x == 0) set_status(D.status, 3, ST_PCG, 0, R_PCG_RZ0); return; }
+    double den = t.b;
+    double beta = 0.0, fin = init, rel = 1.0, mx = 0.0, alpha = 0.0;
+    int it = 0, conv = 0;
+    for (it = 1; it <= D.max_iter; ++it) {
+        if (fabs(den) <= 1.0e-300 || !isfinite(den)) { if (b == 0 && threadIdx.x == 0) set_status(D.status, 3, ST_PCG, it, R_PCG_PAP); return; }
+        alpha = gam / den;
+        const int po = (it - 1) & 1, pn = it & 1;
+        // stage z_it of the halo: s = w_o + beta*s_o, r = r_o - alpha*s, z = r / dz
+        // (SU halo nodes per thread per round, all their loads issued first)
+        __syncthreads();
+        {
+            constexpr int SU = 4;
+            const double* so = sb[po];
+            const double* wo = wb[po];
+            const double* ro = rb[po];
+            for (int k0 = threadIdx.x; k0 < nh; k0 += SU * PCG_THREADS) {
+                double a[SU], c[SU], e[SU];
+#pragma unroll
+                for (int u = 0; u < SU; ++u) {
+                    const int k = k0 + u * PCG_THREADS;
+                    const int j = k < nh ? hidx[k] : 0;
+                    a[u] = __ldcg(so + j);
+                    c[u] = __ldcg(wo + j);
+                    e[u] = __ldcg(ro + j);
+                }
+#pragma unroll
+                for (int u = 0; u < SU; ++u) {
+                    const int k = k0 + u * PCG_THREADS;
+                    if (k < nh) {
+                        const double sj = fma(beta, a[u], c[u]);
+                        const double rj = fma(-alpha, sj, e[u]);
+                        vh[k] = rj / dzh[k];
+                    }
+                }
+            }
+        }
+        __syncthreads();
+        // own rows: p = z_o + beta*p, s = w + beta*s, x += alpha*p, r -= alpha*s
+#pragma unroll
+        for (int k = 0; k < RMAX; ++k) {
+            const int i = row[k];
+            if (i < 0) continue;
+            const double zo = r[k] / dd[k];
+            p[k] = fr[k] ? fma(beta, p[k], zo) : 0.0;
+            s[k] = fma(beta, s[k], w[k]);
+            if (fr[k]) D.pres[i] = fma(alpha, p[k], D.pres[i]);
+            r[k] = fma(-alpha, s[k], r[k]);
+            rb[pn][i] = r[k];
+            sb[pn][i] = s[k];
+        }
+        offdiag_all(off);
+        Acc6 a6{0.0, 0.0, 0.0, 0.0, 0.0};
+#pragma unroll
+        for (int k = 0; k < RMAX; ++k) {
+            const int i = row[k];
+            if (i < 0) continue;
+            const double zi = r[k] / dd[k];
+            w[k] = fr[k] ? fma(D.pdiag[i], zi, off[k]) : 0.0;
+            wb[pn][i] = w[k];
+            if (fr[k]) {
+                if (!isfinite(r[k])) a6.flag = 1.0;
+                a6.a = fma(r[k], zi, a6.a);
+                a6.b = fma(zi, w[k], a6.b);
+                a6.c = fma(r[k], r[k], a6.c);
+                a6.mx = fmax(a6.mx, fabs(r[k]));
+            }
+        }
+        t = Acc6{0.0, 0.0, 0.0, 0.0, 0.0};
+        if (!grid_allreduce3(a6, D, phase, t)) return;
+        ++phase;
+        fin = sqrt(t.c);
+        mx = t.mx;
+        rel = fin / init;
+        if (cg_converged(D.conv_test, rel, mx, D.rel_tol, D.abs_tol)) { conv = 1; break; }
+        if (t.flag > 0.0) { if (b == 0 && threadIdx.x == 0) set_status(D.status, 4, ST_PCG, it, R_PCG_RESID); return; }
+        const double gn = t.a;
+        if (gn <= 1.0e-300 || !isfinite(gn)) { if (b == 0 && threadIdx.x == 0) set_status(D.status, 3, ST_PCG, it, R_PCG_RZ); return; }
+        beta = gn / gam;
+        den = t.b - beta * gn / alpha;
+        gam = gn;
+    }
+    if (it > D.max_iter) it = D.max_iter;
+    cg_finish(D, it, conv, init, fin, rel, mx);
+    if (!conv && b == 0 && threadIdx.x == 0) set_status(D.status, 2, ST_PCG, it, R_PCG_MAXIT);
+}
+
 // Self-test of the bounded device wait: CTA 0 leaves without arriving, so the
 // other CTAs' barrier waits can only end by running out of their spin limit.
 __global__ void k_barrier_selftest(unsigned* bar, DevStatus* st)
@@ -749,8 +1090,8 @@ void PcgEngine::init(const HostModel& m, const uint8_t* nflag, const double* pfi
     if (ncontrib) CUDA_OK(cudaMemcpy(d_cent, P.cent.data(), static_cast<size_t>(ncontrib) * sizeof(int), cudaMemcpyHostToDevice));
     CUDA_OK(cudaMemset(d_val, 0, static_cast<size_t>(nslots ? nslots : 1) * sizeof(double)));
     const size_t n = static_cast<size_t>(N);
-    d_r = dalloc<double>(n); d_z = dalloc<double>(n); d_pA = dalloc<double>(n);
-    d_pB = dalloc<double>(n); d_q = dalloc<double>(n);
+    d_r = dalloc<double>(2 * n); d_z = dalloc<double>(n); d_pA = dalloc<double>(n);
+    d_pB = dalloc<double>(n); d_q = dalloc<double>(2 * n);
     CUDA_OK(cudaMemset(d_pB, 0, n * sizeof(double)));
     if (mixed) {
         d_val32 = dalloc<float>(static_cast<size_t>(nslots));
@@ -777,12 +1118,16 @@ void PcgEngine::init(const HostModel& m, const uint8_t* nflag, const double* pfi
     variant = 1;
     nblocks = grid_for(reinterpret_cast<const void*>(k_pcg64));
     const int rm[4] = {1, 2, 4, 8};
-    if (kernel_choice == 0 || kernel_choice == 3) {
-        const void* hc[4] = {reinterpret_cast<const void*>(k_pcg64h<1>), reinterpret_cast<const void*>(k_pcg64h<2>),
-                             reinterpret_cast<const void*>(k_pcg64h<4>), reinterpret_cast<const void*>(k_pcg64h<8>)};
+    if (kernel_choice == 0 || kernel_choice == 3 || kernel_choice == 4) {
+        const void* hc3[4] = {reinterpret_cast<const void*>(k_pcg64h<1>), reinterpret_cast<const void*>(k_pcg64h<2>),
+                              reinterpret_cast<const void*>(k_pcg64h<4>), reinterpret_cast<const void*>(k_pcg64h<8>)};
+        const void* hc4[4] = {reinterpret_cast<const void*>(k_pcg64c<1>), reinterpret_cast<const void*>(k_pcg64c<2>),
+                              reinterpret_cast<const void*>(k_pcg64c<4>), reinterpret_cast<const void*>(k_pcg64c<8>)};
+        const int want = kernel_choice == 3 ? 3 : 4;
         for (int c = 0; c < 4 && variant == 1; ++c) {
+            const void* fn = want == 4 ? hc4[c] : hc3[c];
             int per_sm = 0;
-            CUDA_OK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, hc[c], PCG_THREADS, 0));
+            CUDA_OK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, PCG_THREADS, 0));
             int g = sms * (per_sm < 2 ? per_sm : 2);
             if (blocks_override > 0 && blocks_override < g) g = blocks_override;
             if (g > nslices) g = nslices > 0 ? nslices : 1;
@@ -812,12 +1157,12 @@ void PcgEngine::init(const HostModel& m, const uint8_t* nflag, const double* pfi
                 smax = std::max(smax, a1 - a0);
             }
             if (!fits) continue;
-            const size_t smem = static_cast<size_t>(hmax) * 12 + static_cast<size_t>(smax) * 2 + 16;
+            const size_t smem = static_cast<size_t>(hmax) * (want == 4 ? 20 : 12) + static_cast<size_t>(smax) * 2 + 16;
             if (smem > 200 * 1024) continue;
-            CUDA_OK(cudaFuncSetAttribute(hc[c], cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
-            CUDA_OK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, hc[c], PCG_THREADS, smem));
+            CUDA_OK(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
+            CUDA_OK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, PCG_THREADS, smem));
             if (per_sm * sms < g) continue;
-            variant = 3;
+            variant = want;
             rmax = rm[c];
             nblocks = g;
             halo_smem = smem;
@@ -839,7 +1184,7 @@ void PcgEngine::init(const HostModel& m, const uint8_t* nflag, const double* pfi
             if ((per_cta + PCG_WARPS - 1) / PCG_WARPS <= rm[c]) { rmax = rm[c]; nblocks = g; variant = 2; break; }
         }
     }
-    d_part = dalloc<double>(static_cast<size_t>(nblocks) * 4 + 8);
+    d_part = dalloc<double>(static_cast<size_t>(nblocks) * 8 + 16);
     d_bar = dalloc<unsigned>(4);
     d_out = dalloc<CgOut>(1);
     CUDA_OK(cudaMemset(d_bar, 0, 4 * sizeof(unsigned)));
@@ -914,6 +1259,12 @@ cbs3d_status PcgEngine::solve(double* pres, double* rhs1, double* pdiag, int pre
         else if (rmax == 4) fn = reinterpret_cast<const void*>(k_pcg64h<4>);
         else fn = reinterpret_cast<const void*>(k_pcg64h<8>);
         smem = halo_smem;
+    } else if (variant == 4) {
+        if (rmax == 1) fn = reinterpret_cast<const void*>(k_pcg64c<1>);
+        else if (rmax == 2) fn = reinterpret_cast<const void*>(k_pcg64c<2>);
+        else if (rmax == 4) fn = reinterpret_cast<const void*>(k_pcg64c<4>);
+        else fn = reinterpret_cast<const void*>(k_pcg64c<8>);
+        smem = halo_smem;
     }
     if (ev0) CUDA_OK(cudaEventRecord(ev0, st));
     CUDA_OK(cudaLaunchCooperativeKernel(fn, dim3(nblocks), dim3(PCG_THREADS), args, smem, st));
@@ -941,6 +1292,12 @@ cbs3d_status PcgEngine::read_result(cbs3d_cg_result& r, cudaStream_t st)
 
 size_t PcgEngine::bytes_per_iter() const
 {
+    if (variant == 4) {
+        // coefficient per pair entry; per node: r, w, s of the previous
+        // iteration read once for staging (24), r, s, w written (24), pressure
+        // read and written (16), pdiag read (8)
+        return static_cast<size_t>(nnz_offdiag) * 8 + static_cast<size_t>(N) * 72;
+    }
     if (variant == 3) {
         // coefficient per pair entry; per node: halo staging of z and the
         // previous direction (each node is in about one CTA's halo per owner

@@ -49,8 +49,9 @@ struct PcgDev {
 // Owns the device copies of the pattern and the PCG work vectors.
 class PcgEngine {
 public:
-    // kernel_choice: 0 automatic, 1 vectors in global memory, 2 register-resident rows,
-    // 3 register-resident rows with the halo staged in shared memory
+    // kernel_choice: 0 automatic (4, else 3, else 2, else 1), 1 vectors in global memory,
+    // 2 register-resident rows, 3 with the halo staged in shared memory,
+    // 4 as 3 with one grid synchronisation per iteration (Chronopoulos-Gear)
     void init(const HostModel& m, const uint8_t* d_nflag, const double* d_pfix, DevStatus* d_status,
               int device, int blocks_override, bool mixed, int kernel_choice = 0);
     void release();
@@ -69,7 +70,7 @@ public:
 
     bool mixed = false;
     int rmax = 0;            // rows per thread of the register-resident kernels (0: global kernel)
-    int variant = 1;         // 1 global vectors, 2 register rows, 3 register rows + shared-memory halo
+    int variant = 1;         // 1 global vectors, 2 register rows, 3 + shared-memory halo, 4 + one sync per iteration
     size_t halo_smem = 0;    // dynamic shared memory of the halo kernel
     int *d_halo_ptr = nullptr, *d_halo_idx = nullptr;
     unsigned short* d_lcol = nullptr;

@@ -95,7 +95,8 @@ typedef struct cbs3d_options {
     int pcg_blocks;          /* persistent PCG grid size; 0 = one wave of resident CTAs */
     int verbose;
     int time_pcg;            /* time every PCG launch with CUDA events (no graph capture) */
-    int pcg_kernel;          /* 0 automatic, 1 vectors in global memory, 2 register-resident rows */
+    int pcg_kernel;          /* 0 automatic; 1 vectors in global memory, 2 register-resident rows,
+                                3 shared-memory halo, 4 halo + one grid sync per iteration */
 } cbs3d_options;
 
 /* Mirrors ConjugateGradient::Result (include/cbs/linalg/ConjugateGradient.hpp:36-68).
