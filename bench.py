@@ -9,8 +9,18 @@ barrier and a device synchronise; time comes from CUDA events on the
 engine's stream (max over ranks).  Every step streams ~0.9 GB of element
 and node data, far more than the 126 MB L2, so no flush is inserted.
 
-  python bench.py [--gpus N] [--steps K] [--warmup W] [--precision fp64|mixed]
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--precision both|fp64|mixed]
   python bench.py --impl reference ...   # the reference solver on the host cores
+
+`value` is the FP64 engine (the drop-in for the reference's FP64 path); with
+--precision both (the default) the same line carries the mixed engine (FP32
+inner PCG, FP64 defect correction) under "mixed": its steps/s, and its
+relative L2 error on u and p against the FP64 engine after the same steps.
+
+Roofline of the PCG kernel: algorithmic bytes per iteration are the
+element-by-element operator's traffic, 64*E_f + 73*N in FP64 and
+40*E_f + 37*N in FP32 (E_f fluid tets, N nodes), times the iterations one
+launch (one pressure solve) runs, over the launch's CUDA-event duration.
 
 Multi-GPU: the single-case path does not shard (replicas only); each rank
 runs its own replica and `value` is the total steps/s of all ranks.
@@ -40,10 +50,10 @@ N_HEX, RE, JITTER, SEED = 64, 400.0, 0.15, 1234
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--steps", type=int, default=40)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="gpu", choices=["gpu", "reference"])
-    ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
+    ap.add_argument("--precision", default="both", choices=["both", "fp64", "mixed"])
     ap.add_argument("--n", type=int, default=N_HEX, help="hexes per side")
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -115,15 +125,15 @@ def measured_peak():
     return 6650.0, "fallback"
 
 
-def ncu_traffic(n: int):
-    """DRAM bytes per PCG launch from the committed ncu summary, if one exists
-    for this mesh size."""
+def ncu_traffic(kernel: str, n: int):
+    """DRAM bytes (read + write) of one PCG launch from the committed ncu
+    summary, if one exists for this kernel and mesh size."""
     path = os.path.join(ROOT, "profiles", "pcg_traffic.json")
     if not os.path.exists(path):
         return None
     with open(path) as f:
         d = json.load(f)
-    return d.get(str(n))
+    return d.get(kernel, {}).get(str(n))
 
 
 # ----------------------------------------------------------- CPU baseline
@@ -214,28 +224,54 @@ def arm_reference(args):
         dist.destroy_process_group()
 
 
-def arm_gpu(args):
-    from cbs3d import gpu
-    ws, rank, local, dist = dist_init()
-    prec = gpu.MIXED if args.precision == "mixed" else gpu.FP64
-    case = make_case(args.n, ntime=10 ** 6)
-    ctx = gpu.Context(case, precision=prec, device=local, use_graph=False, time_pcg=True)
-    N = ctx.npoin
+def algorithmic_bytes(nelem_fluid: int, npoin: int, mixed: bool) -> int:
+    """Bytes one PCG iteration of the element-by-element Jacobi-PCG moves:
+    per fluid tet 4 int32 connectivity + 6 coefficients, per node p, Ap
+    (written and read), pres and r (read and written), pdiag, new p, plus a
+    one-byte mask -- FP64 64*E_f + 73*N, FP32 inner 40*E_f + 37*N."""
+    return (40 * nelem_fluid + 37 * npoin) if mixed else (64 * nelem_fluid + 73 * npoin)
+
+
+def timed_run(args, ctx, dist):
+    """W warm-up steps, then K steps between barriers; returns the stats of
+    both calls, the max-over-ranks device seconds and the clocks seen."""
     warm = ctx.step(args.warmup)
-    clocks = ClockSampler(local)
+    clocks = ClockSampler(ctx.device)
     barrier(dist)
     st = ctx.step(args.steps)
     barrier(dist)
     sec = dist_max(dist, st.gpu_seconds)
-    clk = clocks.stop()
-    # PCG iterations inside the timed region (the totals are cumulative)
-    its_timed = st.cg_iterations_total - warm.cg_iterations_total
-    value = ws * args.steps / sec
+    return warm, st, sec, clocks.stop()
+
+
+def roofline(st, warm, nelem_fluid, npoin, mixed, n):
     peak, peak_kind = measured_peak()
-    bpi = st.pcg_bytes_per_iter
-    pcg_avg = st.pcg_seconds / max(st.pcg_launches, 1)
-    achieved = its_timed * bpi / st.pcg_seconds / 1e9 if st.pcg_seconds > 0 else None
-    traffic = ncu_traffic(args.n)
+    its = st.cg_iterations_total - warm.cg_iterations_total   # totals are cumulative
+    alg = algorithmic_bytes(nelem_fluid, npoin, mixed)
+    achieved = its * alg / st.pcg_seconds / 1e9 if st.pcg_seconds > 0 else None
+    names = {1: "k_pcg64", 2: "k_pcg64r", 3: "k_pcg64h", 4: "k_pcg64c", 5: "k_pcg32m"}
+    kname = names.get(st.pcg_kernel, "?")
+    return {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+            "frac": achieved / peak if achieved else None, "traffic": ncu_traffic(kname, n),
+            "traffic_unit": "bytes per launch (one pressure solve)",
+            "kernel": f"{kname} (persistent PCG, one launch per pressure solve)",
+            "peak_source": peak_kind, "algorithmic_bytes_per_iteration": alg,
+            "kernel_bytes_per_iteration": st.pcg_bytes_per_iter, "iterations": its,
+            "launches": st.pcg_launches, "avg_launch_ms": 1e3 * st.pcg_seconds / max(st.pcg_launches, 1)}
+
+
+def arm_gpu(args):
+    from cbs3d import gpu
+    ws, rank, local, dist = dist_init()
+    case = make_case(args.n, ntime=10 ** 6)
+    nelem_fluid = case.mesh.nelem          # the cavity is all fluid
+    first = gpu.MIXED if args.precision == "mixed" else gpu.FP64
+    ctx = gpu.Context(case, precision=first, device=local, use_graph=False, time_pcg=True)
+    N = ctx.npoin
+    warm, st, sec, clk = timed_run(args, ctx, dist)
+    value = ws * args.steps / sec
+    roof = roofline(st, warm, nelem_fluid, N, first == gpu.MIXED, args.n)
+    u0, p0, _ = ctx.fields()
 
     # end to end through the public API with host buffers: upload the state,
     # one step, download the state, every step
@@ -257,6 +293,24 @@ def arm_gpu(args):
         el = dist_max(dist, time.perf_counter() - t0)
         e2e = {"value": ws * args.e2e_steps / el, "unit": "steps/s", "h2d_bytes_per_step": 5 * N * 8,
                "d2h_bytes_per_step": 5 * N * 8}
+    launches = int(st.kernel_launches)
+    its_per_step = roof["iterations"] / args.steps
+    pcg_share = st.pcg_seconds / st.gpu_seconds if st.gpu_seconds > 0 else None
+    ctx.close()
+
+    mixed = None
+    if args.precision == "both":
+        mctx = gpu.Context(case, precision=gpu.MIXED, device=local, use_graph=False, time_pcg=True)
+        mwarm, mst, msec, _ = timed_run(args, mctx, dist)
+        um, pm, _ = mctx.fields()
+        mixed = {"value": ws * args.steps / msec, "unit": "steps/s", "ms_per_step": 1e3 * msec / args.steps,
+                 "speedup_vs_fp64": (ws * args.steps / msec) / value,
+                 "rel_l2_u_vs_fp64": float(np.linalg.norm(um - u0) / np.linalg.norm(u0)),
+                 "rel_l2_p_vs_fp64": float(np.linalg.norm(pm - p0) / np.linalg.norm(p0)),
+                 "pcg_iterations_per_step": (mst.cg_iterations_total - mwarm.cg_iterations_total) / args.steps,
+                 "roofline": roofline(mst, mwarm, nelem_fluid, N, True, args.n)}
+        launches += int(mst.kernel_launches)
+        mctx.close()
 
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
@@ -266,22 +320,19 @@ def arm_gpu(args):
         line = {
             "metric": METRIC, "value": value, "unit": "steps/s", "n_gpus": ws, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": 1e3 * sec / args.steps, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f64" if prec == gpu.FP64 else "f32+f64",
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64" if first == gpu.FP64 else "f32+f64",
             "data": "synthetic",
-            "config": {"workload": workload(args.n), "nelem": ctx.nelem, "npoin": N,
-                       "precision": args.precision, "l2": "inputs larger than L2 (no flush)",
+            "config": {"workload": workload(args.n), "nelem": case.mesh.nelem, "npoin": N,
+                       "precision": "fp64" if first == gpu.FP64 else "mixed",
+                       "l2": "inputs larger than L2 (no flush): each step streams the element arrays, "
+                             "about 0.6 GB at 64^3",
                        "parallelism": "replicas" if ws > 1 else "single"},
-            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                         "frac": achieved / peak if achieved else None, "traffic": traffic,
-                         "kernel": "k_pcg64 (persistent PCG solve)", "peak_source": peak_kind,
-                         "bytes_per_iteration": bpi, "iterations": its_timed, "launches": st.pcg_launches,
-                         "avg_launch_ms": 1e3 * pcg_avg},
-            "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": int(st.kernel_launches), "clocks": clk,
-            "pcg_iterations_per_step": its_timed / args.steps,
-            "pcg_share_of_step": st.pcg_seconds / st.gpu_seconds if st.gpu_seconds > 0 else None,
+            "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches, "clocks": clk,
+            "pcg_iterations_per_step": its_per_step, "pcg_share_of_step": pcg_share,
         }
+        if mixed is not None:
+            line["mixed"] = mixed
         print(json.dumps(line))
-    ctx.close()
     if dist is not None:
         barrier(dist)
         dist.destroy_process_group()

@@ -97,7 +97,8 @@ class StepStats(ctypes.Structure):
     _fields_ = [("steps_done", _i), ("iitime", _i), ("failed_step", _i), ("dtreal", _d), ("rtime", _d),
                 ("cg", CGResult), ("cg_iterations_total", ctypes.c_longlong), ("hb", _d * 15),
                 ("gpu_seconds", _d), ("steady_reached", _i), ("pcg_seconds", _d), ("pcg_launches", _i),
-                ("kernel_launches", ctypes.c_longlong), ("pcg_bytes_per_iter", _d)]
+                ("kernel_launches", ctypes.c_longlong), ("pcg_bytes_per_iter", _d),
+                ("pcg_kernel", _i)]
 
 
 # case-generator parameter names -> cbs3d_params fields
@@ -198,6 +199,7 @@ class Context:
                  pcg_kernel: int = 0):
         L = lib()
         self.h = ctypes.c_void_p()
+        self.device = device
         err = ctypes.create_string_buffer(1024)
         opt = make_options(precision, device, inner_tol, use_graph, pcg_blocks, time_pcg, pcg_kernel)
         if case_name is not None:

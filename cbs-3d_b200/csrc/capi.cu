@@ -336,9 +336,10 @@ void cbs3d_ctx::enqueue_step(int it)
     k_conv_partial<<<static_cast<unsigned>(conv_blocks), T, 0, st>>>(S);
     k_conv_finish<<<1, 15 * 32, 0, st>>>(S, conv_blocks);
     k_step_log<<<1, 32, 0, st>>>(S, pcg.d_out, d_log, d_counter, log_cap);
-    // begin, timestep, dt_finish, lhs, step1 x2, step2 x2, assemble, impose, pcg, step3 x2, conv x2, log
-    step_kernels = 17 + (!fixed_dt(it) && force_global() ? 1 : 0) + (m.p.step2_check > 0 ? 2 : 0) +
-                   (m.temp_calc > 0 ? 2 : 0) + (pcg.mixed ? pcg.extra_launches_per_solve() : 0);
+    // begin, timestep, dt_finish, lhs, step1 x2, step2 x2, assemble, step3 x2, conv x2, log (14)
+    // plus the pressure solve's launches
+    step_kernels = 14 + pcg.launches_per_solve() + (!fixed_dt(it) && force_global() ? 1 : 0) +
+                   (m.p.step2_check > 0 ? 2 : 0) + (m.temp_calc > 0 ? 2 : 0);
 }
 
 void cbs3d_ctx::ensure_log(int n)
@@ -572,6 +573,7 @@ cbs3d_status cbs3d_step(cbs3d_ctx* c, int nsteps, int stop_on_steady, cbs3d_step
             stats->cg_iterations_total = c->cg_total;
             stats->kernel_launches = c->launches - launches0;
             stats->pcg_bytes_per_iter = static_cast<double>(c->pcg.bytes_per_iter());
+            stats->pcg_kernel = c->pcg.variant == 4 && c->pcg.mixed_ok ? 5 : c->pcg.variant;
             for (int k = 0; k + 1 < c->pcg_ev_used; k += 2) {
                 float pm = 0.0f;
                 CUDA_OK(cudaEventElapsedTime(&pm, c->pcg_ev[static_cast<size_t>(k)], c->pcg_ev[static_cast<size_t>(k) + 1]));
@@ -834,7 +836,7 @@ cbs3d_status cbs3d_pcg_create(int nelem, int npoin, const int* intma, const int*
         for (int v : m.intma)
             if (v < 1 || v > npoin) throw Error(CBS3D_INVALID_INPUT, "ConjugateGradient::solvePressure - element connectivity node out of range");
         build_incidence(m.intma, npoin, m.n2e_ptr, m.n2e);
-        build_pressure_pattern(m.intma, m.mat, npoin, m.n2e_ptr, m.n2e, m.pat);
+        build_pressure_pattern(m.intma, m.mat, npoin, m.n2e_ptr, m.n2e, m.pat, nullptr);
         // build_pressure_active_mask / build_fixed_pressure_mask (src/linalg/ConjugateGradient.cpp:98-177)
         std::vector<uint8_t> nflag(static_cast<size_t>(npoin), 0);
         std::vector<double> pfix(static_cast<size_t>(npoin), 0.0);

@@ -527,85 +527,133 @@ void build_incidence(const std::vector<int>& intma, int N, std::vector<int>& ptr
         for (int a = 0; a < 4; ++a) idx[static_cast<size_t>(fill[static_cast<size_t>(intma[4 * e + a] - 1)]++)] = static_cast<int>(4 * e + a);
 }
 
-// Pattern of the assembled pressure operator (see PressurePattern).
+// Row order of the pressure operator: nodes sorted along a Morton curve of
+// their coordinates (identity without coordinates), so that the rows of one
+// slice, and of one CTA's block of slices, are spatially compact and their
+// neighbour sets (halos) small.  The order only groups rows; every row's
+// entries and their contributions are unchanged.
+std::vector<int> locality_order(const double* coord, int N)
+{
+    std::vector<int> ord(static_cast<size_t>(N));
+    for (int i = 0; i < N; ++i) ord[static_cast<size_t>(i)] = i;
+    if (!coord || N < 2) return ord;
+    double lo[3] = {coord[0], coord[1], coord[2]}, hi[3] = {coord[0], coord[1], coord[2]};
+    for (int i = 0; i < N; ++i)
+        for (int d = 0; d < 3; ++d) {
+            lo[d] = std::min(lo[d], coord[3 * static_cast<size_t>(i) + d]);
+            hi[d] = std::max(hi[d], coord[3 * static_cast<size_t>(i) + d]);
+        }
+    auto spread = [](unsigned long long v) {   // 21 bits -> every third bit
+        v &= 0x1fffffULL;
+        v = (v | v << 32) & 0x1f00000000ffffULL;
+        v = (v | v << 16) & 0x1f0000ff0000ffULL;
+        v = (v | v << 8) & 0x100f00f00f00f00fULL;
+        v = (v | v << 4) & 0x10c30c30c30c30c3ULL;
+        v = (v | v << 2) & 0x1249249249249249ULL;
+        return v;
+    };
+    std::vector<unsigned long long> key(static_cast<size_t>(N));
+    for (int i = 0; i < N; ++i) {
+        unsigned long long k = 0;
+        for (int d = 0; d < 3; ++d) {
+            const double span = hi[d] - lo[d];
+            const double t = span > 0.0 ? (coord[3 * static_cast<size_t>(i) + d] - lo[d]) / span : 0.0;
+            const unsigned long long q = static_cast<unsigned long long>(t * 2097151.0 + 0.5);
+            k |= spread(q) << d;
+        }
+        key[static_cast<size_t>(i)] = k;
+    }
+    std::stable_sort(ord.begin(), ord.end(), [&](int x, int y) { return key[static_cast<size_t>(x)] < key[static_cast<size_t>(y)]; });
+    return ord;
+}
+
+// Pattern of the assembled pressure operator (see PressurePattern); row
+// position p holds node order[p].
 void build_pressure_pattern(const std::vector<int>& intma, const std::vector<int>& mat, int N,
                             const std::vector<int>& n2e_ptr, const std::vector<int>& n2e,
-                            PressurePattern& pat)
+                            PressurePattern& pat, const double* coord)
 {
     const size_t Ns = static_cast<size_t>(N);
-
-        static const int PAIR[4][4] = {{-1, 0, 1, 2}, {0, -1, 3, 4}, {1, 3, -1, 5}, {2, 4, 5, -1}};
-        pat = PressurePattern{};
-        pat.nslices = (N + 31) / 32;
-        pat.slice_off.assign(static_cast<size_t>(pat.nslices) + 1, 0);
-        pat.slice_w.assign(static_cast<size_t>(pat.nslices), 0);
-        // per row: sorted unique neighbour list and contributions
-        std::vector<int> row_len(Ns, 0);
-        std::vector<std::pair<int, int>> items;
-        // first pass: row lengths
-        auto row_items = [&](size_t i, std::vector<std::pair<int, int>>& it) {
-            it.clear();
-            for (int k = n2e_ptr[i]; k < n2e_ptr[i + 1]; ++k) {
-                const int slot = n2e[k];
-                const size_t e = static_cast<size_t>(slot >> 2);
-                const int a = slot & 3;
-                if (mat[e] != 0) continue;
-                for (int b = 0; b < 4; ++b) {
-                    if (b == a) continue;
-                    it.emplace_back(intma[4 * e + b] - 1, static_cast<int>(e * 8 + PAIR[a][b]));
+    static const int PAIR[4][4] = {{-1, 0, 1, 2}, {0, -1, 3, 4}, {1, 3, -1, 5}, {2, 4, 5, -1}};
+    pat = PressurePattern{};
+    const std::vector<int> order = locality_order(coord, N);
+    pat.nslices = (N + 31) / 32;
+    pat.row_node.assign(static_cast<size_t>(pat.nslices) * 32, -1);
+    for (size_t q = 0; q < Ns; ++q) pat.row_node[q] = order[q];
+    pat.slice_off.assign(static_cast<size_t>(pat.nslices) + 1, 0);
+    pat.slice_w.assign(static_cast<size_t>(pat.nslices), 0);
+    std::vector<int> row_len(Ns, 0);
+    std::vector<std::pair<int, int>> items;
+    // (column, e*8 + pair) of node i's fluid pair entries, stable-sorted by
+    // column so each column keeps ascending element order
+    auto row_items = [&](size_t i, std::vector<std::pair<int, int>>& it) {
+        it.clear();
+        for (int k = n2e_ptr[i]; k < n2e_ptr[i + 1]; ++k) {
+            const int slot = n2e[k];
+            const size_t e = static_cast<size_t>(slot >> 2);
+            const int a = slot & 3;
+            if (mat[e] != 0) continue;
+            for (int b = 0; b < 4; ++b) {
+                if (b == a) continue;
+                it.emplace_back(intma[4 * e + b] - 1, static_cast<int>(e * 8 + PAIR[a][b]));
+            }
+        }
+        std::stable_sort(it.begin(), it.end(), [](const std::pair<int, int>& x, const std::pair<int, int>& y) {
+            return x.first < y.first;
+        });
+    };
+    for (size_t i = 0; i < Ns; ++i) {
+        row_items(i, items);
+        int len = 0;
+        for (size_t q = 0; q < items.size(); ++q)
+            if (q == 0 || items[q].first != items[q - 1].first) ++len;
+        row_len[i] = len;
+        pat.max_row = std::max(pat.max_row, len);
+    }
+    long long off = 0;
+    for (int s = 0; s < pat.nslices; ++s) {
+        int w = 0;
+        for (int l = 0; l < 32; ++l) {
+            const int i = pat.row_node[static_cast<size_t>(s) * 32 + l];
+            if (i >= 0) w = std::max(w, row_len[static_cast<size_t>(i)]);
+        }
+        pat.slice_w[static_cast<size_t>(s)] = w;
+        pat.slice_off[static_cast<size_t>(s)] = off;
+        off += 32LL * w;
+    }
+    pat.slice_off[static_cast<size_t>(pat.nslices)] = off;
+    pat.nslots = off;
+    if (off > 0x7fffffffLL) bad("pressure operator pattern exceeds 2^31 slots");
+    // padding slots point at the row's own node (coefficient 0)
+    pat.col.assign(static_cast<size_t>(off), 0);
+    std::vector<long long> slot_cnt(static_cast<size_t>(off), 0);
+    for (int s = 0; s < pat.nslices; ++s)
+        for (int l = 0; l < 32; ++l) {
+            const int i = pat.row_node[static_cast<size_t>(s) * 32 + l];
+            const long long base = pat.slice_off[static_cast<size_t>(s)] + l;
+            int k = -1;
+            if (i >= 0) {
+                row_items(static_cast<size_t>(i), items);
+                for (size_t q = 0; q < items.size(); ++q) {
+                    if (q == 0 || items[q].first != items[q - 1].first) ++k;
+                    const size_t slot = static_cast<size_t>(base + 32LL * k);
+                    pat.col[slot] = items[q].first;
+                    ++slot_cnt[slot];
                 }
             }
-            // stable sort by column keeps ascending element order per column
-            std::stable_sort(it.begin(), it.end(), [](const std::pair<int, int>& x, const std::pair<int, int>& y) {
-                return x.first < y.first;
-            });
-        };
-        for (size_t i = 0; i < Ns; ++i) {
-            row_items(i, items);
-            int len = 0;
-            for (size_t q = 0; q < items.size(); ++q)
-                if (q == 0 || items[q].first != items[q - 1].first) ++len;
-            row_len[i] = len;
-            pat.max_row = std::max(pat.max_row, len);
+            for (int kk = k + 1; kk < pat.slice_w[static_cast<size_t>(s)]; ++kk)
+                pat.col[static_cast<size_t>(base + 32LL * kk)] = i >= 0 ? i : 0;
         }
-        long long off = 0;
-        for (int s = 0; s < pat.nslices; ++s) {
-            int w = 0;
-            for (int l = 0; l < 32; ++l) {
-                const size_t i = static_cast<size_t>(s) * 32 + l;
-                if (i < Ns) w = std::max(w, row_len[i]);
-            }
-            pat.slice_w[static_cast<size_t>(s)] = w;
-            pat.slice_off[static_cast<size_t>(s)] = off;
-            off += 32LL * w;
-        }
-        pat.slice_off[static_cast<size_t>(pat.nslices)] = off;
-        pat.nslots = off;
-        if (off > 0x7fffffffLL) bad("pressure operator pattern exceeds 2^31 slots");
-        pat.col.assign(static_cast<size_t>(off), 0);
-        std::vector<long long> slot_cnt(static_cast<size_t>(off), 0);
-        // second pass: columns and contribution counts
-        for (size_t i = 0; i < Ns; ++i) {
-            const size_t s = i / 32, l = i % 32;
-            const long long base = pat.slice_off[s] + static_cast<long long>(l);
-            row_items(i, items);
-            int k = -1;
-            for (size_t q = 0; q < items.size(); ++q) {
-                if (q == 0 || items[q].first != items[q - 1].first) ++k;
-                const size_t slot = static_cast<size_t>(base + 32LL * k);
-                pat.col[slot] = items[q].first;
-                ++slot_cnt[slot];
-            }
-            for (int kk = k + 1; kk < pat.slice_w[s]; ++kk) pat.col[static_cast<size_t>(base + 32LL * kk)] = static_cast<int>(i);
-        }
-        pat.cptr.assign(static_cast<size_t>(off) + 1, 0);
-        for (size_t q = 0; q < static_cast<size_t>(off); ++q) pat.cptr[q + 1] = pat.cptr[q] + slot_cnt[q];
-        pat.cent.assign(static_cast<size_t>(pat.cptr[static_cast<size_t>(off)]), 0);
-        std::vector<long long> fillp(pat.cptr.begin(), pat.cptr.end() - 1);
-        for (size_t i = 0; i < Ns; ++i) {
-            const size_t s = i / 32, l = i % 32;
-            const long long base = pat.slice_off[s] + static_cast<long long>(l);
-            row_items(i, items);
+    pat.cptr.assign(static_cast<size_t>(off) + 1, 0);
+    for (size_t q = 0; q < static_cast<size_t>(off); ++q) pat.cptr[q + 1] = pat.cptr[q] + slot_cnt[q];
+    pat.cent.assign(static_cast<size_t>(pat.cptr[static_cast<size_t>(off)]), 0);
+    std::vector<long long> fillp(pat.cptr.begin(), pat.cptr.end() - 1);
+    for (int s = 0; s < pat.nslices; ++s)
+        for (int l = 0; l < 32; ++l) {
+            const int i = pat.row_node[static_cast<size_t>(s) * 32 + l];
+            if (i < 0) continue;
+            const long long base = pat.slice_off[static_cast<size_t>(s)] + l;
+            row_items(static_cast<size_t>(i), items);
             int k = -1;
             for (size_t q = 0; q < items.size(); ++q) {
                 if (q == 0 || items[q].first != items[q - 1].first) ++k;
@@ -613,7 +661,7 @@ void build_pressure_pattern(const std::vector<int>& intma, const std::vector<int
                 pat.cent[static_cast<size_t>(fillp[slot]++)] = items[q].second;
             }
         }
-    }
+}
 
 // ----------------------------------------------------------------- build
 void HostModel::build()
@@ -915,7 +963,7 @@ void HostModel::build()
     }
 
     // ------------------------------------------ pressure-operator pattern
-    build_pressure_pattern(intma, mat, N, n2e_ptr, n2e, pat);
+    build_pressure_pattern(intma, mat, N, n2e_ptr, n2e, pat, coord.data());
 
     // Initial boundary values: Boundary::applyTemperature, applyVelocity,
     // applyPressure (src/solver/Solver.cpp:297-299).

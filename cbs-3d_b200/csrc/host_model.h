@@ -40,6 +40,7 @@ enum { VBC_FIXED = 1, VBC_SOLID = 2 };
 struct PressurePattern {
     int nslices = 0;
     long long nslots = 0;
+    std::vector<int> row_node;           // nslices*32: node of each row position (-1 padding)
     std::vector<long long> slice_off;    // nslices+1, slot offsets
     std::vector<int> slice_w;            // nslices, slots per row in the slice
     std::vector<int> col;                // nslots (0-based node)
@@ -98,8 +99,9 @@ void default_params(cbs3d_params& p);
 
 // Node -> (element, local node) incidence in element order; slot = e*4 + a.
 void build_incidence(const std::vector<int>& intma, int N, std::vector<int>& ptr, std::vector<int>& idx);
+// coord (3N, may be NULL) orders the rows along a Morton curve for locality.
 void build_pressure_pattern(const std::vector<int>& intma, const std::vector<int>& mat, int N,
                             const std::vector<int>& n2e_ptr, const std::vector<int>& n2e,
-                            PressurePattern& pat);
+                            PressurePattern& pat, const double* coord);
 
 }  // namespace cbs3d

@@ -79,7 +79,7 @@ __global__ void k_ell_from_gstif(const double* gstif, const long long* cptr, con
 __global__ void k_impose(PcgDev D)
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= D.N) return;
+    if (i >= D.NN) return;
     const uint8_t f = D.nflag[i];
     if (!(f & 1)) {
         D.pres[i] = 0.0; D.rhs1[i] = 0.0; D.pdiag[i] = 0.0;
@@ -88,16 +88,43 @@ __global__ void k_impose(PcgDev D)
     }
 }
 
+// Node order -> row-position order of the solver's inputs, and back for the
+// pressure.  Padding positions get inactive flags and zeros.
+__global__ void k_perm_in(PcgDev D, const double* pres, const double* rhs1, const double* pdiag,
+                          const uint8_t* nflag, double* xp, double* bp, double* dp, uint8_t* fp)
+{
+    const int pos = blockIdx.x * blockDim.x + threadIdx.x;
+    if (pos >= D.N) return;
+    const int i = D.row_node[pos];
+    xp[pos] = i >= 0 ? pres[i] : 0.0;
+    bp[pos] = i >= 0 ? rhs1[i] : 0.0;
+    dp[pos] = i >= 0 ? pdiag[i] : 0.0;
+    fp[pos] = i >= 0 ? (uint8_t)(nflag[i] & 5) : (uint8_t)0;
+}
+
+__global__ void k_perm_out(PcgDev D, const double* xp, double* pres)
+{
+    const int pos = blockIdx.x * blockDim.x + threadIdx.x;
+    if (pos >= D.N) return;
+    const int i = D.row_node[pos];
+    if (i >= 0) pres[i] = xp[pos];
+}
+
 // y = A x on the assembled operator; identity rows on fixed nodes
 __global__ void k_ell_multiply(PcgDev D, const double* x, double* y)
 {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= D.N) return;
-    const int s = i >> 5, lane = i & 31;
+    const int pos = blockIdx.x * blockDim.x + threadIdx.x;
+    if (pos >= D.nslices * 32) return;
+    const int i = D.row_node[pos];
+    if (i < 0) return;
+    const int s = pos >> 5, lane = pos & 31;
     const long long base = D.slice_off[s] + lane;
     const int w = D.slice_w[s];
     double off = 0.0;
-    for (int k = 0; k < w; ++k) off = fma(D.val[base + 32LL * k], x[D.col[base + 32LL * k]], off);
+    for (int k = 0; k < w; ++k) {
+        const int j = D.row_node[D.col[base + 32LL * k]];
+        off = fma(D.val[base + 32LL * k], j >= 0 ? x[j] : 0.0, off);
+    }
     double v = fma(D.pdiag[i], x[i], off);
     if (D.nflag[i] & 4) v = x[i];
     y[i] = v;
@@ -219,13 +246,12 @@ __global__ void __launch_bounds__(PCG_THREADS) k_pcg64(PcgDev D)
     const int s_beg = (int)((long long)b * D.nslices / G);
     const int s_end = (int)((long long)(b + 1) * D.nslices / G);
     int phase = 0;
-    const int N = D.N;
+    
 
     // ---- r0 = b - A p0, z0, d0 = z0, (r,r), (r,z), max|r|
     Acc4 acc{0.0, 0.0, 0.0, 0.0};
     for (int s = s_beg + warp; s < s_end; s += PCG_WARPS) {
         const int i = s * 32 + lane;
-        if (i >= N) continue;
         const long long base = D.slice_off[s] + lane;
         const int w = D.slice_w[s];
         double off = 0.0;
@@ -274,7 +300,6 @@ __global__ void __launch_bounds__(PCG_THREADS) k_pcg64(PcgDev D)
         const bool upd = it > 1;
         for (int s = s_beg + warp; s < s_end; s += PCG_WARPS) {
             const int i = s * 32 + lane;
-            if (i >= N) continue;
             const long long base = D.slice_off[s] + lane;
             const int w = D.slice_w[s];
             const uint8_t f = D.nflag[i];
@@ -306,7 +331,6 @@ __global__ void __launch_bounds__(PCG_THREADS) k_pcg64(PcgDev D)
         Acc4 rr{0.0, 0.0, 0.0, 0.0};
         for (int s = s_beg + warp; s < s_end; s += PCG_WARPS) {
             const int i = s * 32 + lane;
-            if (i >= N) continue;
             const uint8_t f = D.nflag[i];
             if (!((f & 1) && !(f & 4))) continue;
             D.pres[i] = fma(alpha, pc[i], D.pres[i]);
@@ -354,7 +378,7 @@ __global__ void __launch_bounds__(PCG_THREADS, 2) k_pcg64r(PcgDev D)
     const int s_beg = (int)((long long)b * D.nslices / G);
     const int s_end = (int)((long long)(b + 1) * D.nslices / G);
     int phase = 0;
-    const int N = D.N;
+    
 
     double r[RMAX], p[RMAX], q[RMAX], dg[RMAX];
     bool fr[RMAX];
@@ -363,7 +387,6 @@ __global__ void __launch_bounds__(PCG_THREADS, 2) k_pcg64r(PcgDev D)
     for (int k = 0; k < RMAX; ++k) {
         const int s = s_beg + warp + PCG_WARPS * k;
         row[k] = (s < s_end) ? s * 32 + lane : -1;
-        if (row[k] >= N) row[k] = -1;
         r[k] = p[k] = q[k] = dg[k] = 0.0;
         fr[k] = false;
     }
@@ -543,7 +566,7 @@ __global__ void __launch_bounds__(PCG_THREADS, 2) k_pcg64h(PcgDev D)
     for (int k = threadIdx.x; k < nh; k += PCG_THREADS) hidx[k] = D.halo_idx[h0 + k];
     for (int k = threadIdx.x; k < nsl; k += PCG_THREADS) lcs[k] = D.lcol[S0 + k];
     int phase = 0;
-    const int N = D.N;
+    
 
     double r[RMAX], p[RMAX], q[RMAX], dg[RMAX];
     bool fr[RMAX];
@@ -560,7 +583,6 @@ __global__ void __launch_bounds__(PCG_THREADS, 2) k_pcg64h(PcgDev D)
             wr[k] = D.slice_w[s];
             wmax = wr[k] > wmax ? wr[k] : wmax;
         }
-        if (row[k] >= N) row[k] = -1;
         r[k] = p[k] = q[k] = dg[k] = 0.0;
         fr[k] = false;
     }
@@ -710,33 +732,43 @@ struct Acc6 {
     double a, b, c, mx, flag;
 };
 
-__device__ __forceinline__ bool grid_allreduce3(Acc6 v, const PcgDev& D, int phase, Acc6& out)
+// Grid-wide all-reduce of NV values per thread: the first NSUM summed, the
+// rest max-reduced.  Fixed reduction tree (warp shuffles, warps in order,
+// CTAs by index in the last-arriving CTA), so the result is deterministic.
+// Returns false when the barrier gave up or another CTA raised a status.
+template <int NV, int NSUM>
+__device__ __forceinline__ bool grid_allreduce_v(double (&v)[NV], const PcgDev& D, int phase, double (&out)[NV])
 {
-    __shared__ double sm[PCG_WARPS][5];
-    __shared__ double tot[5];
+    static_assert(NV <= 8, "partials hold 8 doubles per CTA");
+    __shared__ double sm[PCG_WARPS][NV];
+    __shared__ double tot[NV];
     __shared__ int s_last, s_ok;
     const int G = gridDim.x;
-    for (int o = 16; o > 0; o >>= 1) {
-        v.a += __shfl_down_sync(0xffffffffu, v.a, o);
-        v.b += __shfl_down_sync(0xffffffffu, v.b, o);
-        v.c += __shfl_down_sync(0xffffffffu, v.c, o);
-        v.mx = fmax(v.mx, __shfl_down_sync(0xffffffffu, v.mx, o));
-        v.flag = fmax(v.flag, __shfl_down_sync(0xffffffffu, v.flag, o));
-    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1)
+#pragma unroll
+        for (int q = 0; q < NV; ++q) {
+            const double x = __shfl_down_sync(0xffffffffu, v[q], o);
+            v[q] = q < NSUM ? v[q] + x : fmax(v[q], x);
+        }
     const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    if (lane == 0) { sm[w][0] = v.a; sm[w][1] = v.b; sm[w][2] = v.c; sm[w][3] = v.mx; sm[w][4] = v.flag; }
+    if (lane == 0)
+#pragma unroll
+        for (int q = 0; q < NV; ++q) sm[w][q] = v[q];
     __syncthreads();
     unsigned* cnt = D.bar;
     unsigned* gen = D.bar + 1;
     double* totals = D.part + (size_t)G * 8 + (size_t)(phase & 1) * 8;
     if (threadIdx.x == 0) {
-        double t[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
-        for (int k = 0; k < PCG_WARPS; ++k) {
-            t[0] += sm[k][0]; t[1] += sm[k][1]; t[2] += sm[k][2];
-            t[3] = fmax(t[3], sm[k][3]); t[4] = fmax(t[4], sm[k][4]);
-        }
+        double t[NV];
+#pragma unroll
+        for (int q = 0; q < NV; ++q) t[q] = 0.0;
+        for (int k = 0; k < PCG_WARPS; ++k)
+#pragma unroll
+            for (int q = 0; q < NV; ++q) t[q] = q < NSUM ? t[q] + sm[k][q] : fmax(t[q], sm[k][q]);
         double* p = D.part + (size_t)blockIdx.x * 8;
-        for (int k = 0; k < 5; ++k) __stcg(p + k, t[k]);
+#pragma unroll
+        for (int q = 0; q < NV; ++q) __stcg(p + q, t[q]);
         const unsigned g = ld_acquire(gen);
         unsigned arrived;
         asm volatile("atom.add.acq_rel.gpu.global.u32 %0, [%1], 1;" : "=r"(arrived) : "l"(cnt) : "memory");
@@ -753,43 +785,73 @@ __device__ __forceinline__ bool grid_allreduce3(Acc6 v, const PcgDev& D, int pha
                 }
                 __nanosleep(20);
             }
-            if (s_ok) for (int k = 0; k < 5; ++k) tot[k] = __ldcg(totals + k);
+            if (s_ok)
+#pragma unroll
+                for (int q = 0; q < NV; ++q) tot[q] = __ldcg(totals + q);
         }
     }
     __syncthreads();
     if (s_last) {
-        double t[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
+        double t[NV];
+#pragma unroll
+        for (int q = 0; q < NV; ++q) t[q] = 0.0;
         for (int k = threadIdx.x; k < G; k += PCG_THREADS) {
             const double* p = D.part + (size_t)k * 8;
-            t[0] += __ldcg(p); t[1] += __ldcg(p + 1); t[2] += __ldcg(p + 2);
-            t[3] = fmax(t[3], __ldcg(p + 3)); t[4] = fmax(t[4], __ldcg(p + 4));
+#pragma unroll
+            for (int q = 0; q < NV; ++q) t[q] = q < NSUM ? t[q] + __ldcg(p + q) : fmax(t[q], __ldcg(p + q));
         }
-        for (int o = 16; o > 0; o >>= 1) {
-            t[0] += __shfl_down_sync(0xffffffffu, t[0], o);
-            t[1] += __shfl_down_sync(0xffffffffu, t[1], o);
-            t[2] += __shfl_down_sync(0xffffffffu, t[2], o);
-            t[3] = fmax(t[3], __shfl_down_sync(0xffffffffu, t[3], o));
-            t[4] = fmax(t[4], __shfl_down_sync(0xffffffffu, t[4], o));
-        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1)
+#pragma unroll
+            for (int q = 0; q < NV; ++q) {
+                const double x = __shfl_down_sync(0xffffffffu, t[q], o);
+                t[q] = q < NSUM ? t[q] + x : fmax(t[q], x);
+            }
         __syncthreads();
-        if (lane == 0) for (int k = 0; k < 5; ++k) sm[w][k] = t[k];
+        if (lane == 0)
+#pragma unroll
+            for (int q = 0; q < NV; ++q) sm[w][q] = t[q];
         __syncthreads();
         if (threadIdx.x == 0) {
-            double u[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
-            for (int k = 0; k < PCG_WARPS; ++k) {
-                u[0] += sm[k][0]; u[1] += sm[k][1]; u[2] += sm[k][2];
-                u[3] = fmax(u[3], sm[k][3]); u[4] = fmax(u[4], sm[k][4]);
-            }
-            for (int k = 0; k < 5; ++k) { tot[k] = u[k]; __stcg(totals + k, u[k]); }
+            double u[NV];
+#pragma unroll
+            for (int q = 0; q < NV; ++q) u[q] = 0.0;
+            for (int k = 0; k < PCG_WARPS; ++k)
+#pragma unroll
+                for (int q = 0; q < NV; ++q) u[q] = q < NSUM ? u[q] + sm[k][q] : fmax(u[q], sm[k][q]);
+#pragma unroll
+            for (int q = 0; q < NV; ++q) { tot[q] = u[q]; __stcg(totals + q, u[q]); }
             atomicExch(cnt, 0u);
             asm volatile("red.release.gpu.global.add.u32 [%0], 1;" :: "l"(gen) : "memory");
             if (ld_relaxed_int(&D.status->code) != 0) s_ok = 0;
         }
     }
     __syncthreads();
-    out = Acc6{tot[0], tot[1], tot[2], tot[3], tot[4]};
+#pragma unroll
+    for (int q = 0; q < NV; ++q) out[q] = tot[q];
     const bool ok = s_ok != 0;
     __syncthreads();
+    return ok;
+}
+
+__device__ __forceinline__ bool grid_allreduce3(Acc6 v, const PcgDev& D, int phase, Acc6& out)
+{
+    double a[5] = {v.a, v.b, v.c, v.mx, v.flag}, o[5];
+    const bool ok = grid_allreduce_v<5, 3>(a, D, phase, o);
+    out = Acc6{o[0], o[1], o[2], o[3], o[4]};
+    return ok;
+}
+
+// Five sums, a max and a flag (the mixed solver's refresh after a correction).
+struct Acc8 {
+    double a, b, c, d, e, mx, flag;
+};
+
+__device__ __forceinline__ bool grid_allreduce5(Acc8 v, const PcgDev& D, int phase, Acc8& out)
+{
+    double a[7] = {v.a, v.b, v.c, v.d, v.e, v.mx, v.flag}, o[7];
+    const bool ok = grid_allreduce_v<7, 5>(a, D, phase, o);
+    out = Acc8{o[0], o[1], o[2], o[3], o[4], o[5], o[6]};
     return ok;
 }
 
@@ -834,7 +896,6 @@ __global__ void __launch_bounds__(PCG_THREADS, 2) k_pcg64c(PcgDev D)
             wr[k] = D.slice_w[sl];
             wmax = wr[k] > wmax ? wr[k] : wmax;
         }
-        if (row[k] >= N) row[k] = -1;
         r[k] = p[k] = s[k] = w[k] = 0.0;
         dd[k] = __longlong_as_double(0x7ff0000000000000LL);
         fr[k] = false;
@@ -1036,6 +1097,346 @@ __global__ void __launch_bounds__(PCG_THREADS, 2) k_pcg64c(PcgDev D)
     if (!conv && b == 0 && threadIdx.x == 0) set_status(D.status, 2, ST_PCG, it, R_PCG_MAXIT);
 }
 
+// ------------------------------------------- mixed-precision PCG (FP32)
+// The Chronopoulos-Gear iteration of k_pcg64c in FP32 -- r, z, w, s, p and
+// the assembled coefficients are single precision, the coefficients and local
+// column indices resident in shared memory for the whole solve -- with the
+// reductions, alpha/beta and the pressure in FP64, and FP64 defect
+// correction by residual replacement: whenever the recursive residual has
+// fallen by RU_FACTOR since the last correction, and whenever it meets the
+// stopping test, the true residual r = b - A x is recomputed from the FP64
+// coefficients and FP64 pressure, and w = A z, s = A p are recomputed, so the
+// FP32 recurrences restart from exact data without discarding the search
+// direction; the curvature of the next direction is then computed from
+// fresh products rather than recurred, and a correction that finds no
+// progress since the previous one also drops the direction.  The solve
+// stops only when the FP64 true residual meets the reference's stopping
+// test.
+constexpr double RU_FACTOR = 0.05;
+constexpr int RU_STALL = 256;   // iterations without a correction before one is forced
+
+template <int RMAX>
+__global__ void __launch_bounds__(PCG_THREADS, 2) k_pcg32m(PcgDev D)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int G = gridDim.x, b = blockIdx.x;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int s_beg = (int)((long long)b * D.nslices / G);
+    const int s_end = (int)((long long)(b + 1) * D.nslices / G);
+    const long long S0 = D.slice_off[s_beg];
+    const int nsl = (int)(D.slice_off[s_end] - S0);
+    const int h0 = D.halo_ptr[b];
+    const int nh = D.halo_ptr[b + 1] - h0;
+    const int HM = D.halo_max;
+    double* vh64 = reinterpret_cast<double*>(smem_raw);                 // HM doubles, or:
+    float* vz = reinterpret_cast<float*>(smem_raw);                     //   HM floats (z)
+    float* vp = vz + HM;                                                //   HM floats (p)
+    float* dzh = reinterpret_cast<float*>(vh64 + HM);                   // HM
+    int* hidx = reinterpret_cast<int*>(dzh + HM);                       // HM
+    float* val32s = reinterpret_cast<float*>(hidx + HM);                // nsl
+    unsigned short* lcs = reinterpret_cast<unsigned short*>(val32s + D.slot_max);
+    for (int k = threadIdx.x; k < nh; k += PCG_THREADS) hidx[k] = D.halo_idx[h0 + k];
+    for (int k = threadIdx.x; k < nsl; k += PCG_THREADS) {
+        lcs[k] = D.lcol[S0 + k];
+        val32s[k] = D.val32[S0 + k];
+    }
+    int phase = 0;
+    const int N = D.N;
+    float* rb[2] = {D.r32, D.r32 + N};
+    float* wb[2] = {D.w32, D.w32 + N};
+    float* sb[2] = {D.s32, D.s32 + N};
+    float* pb = D.p32;
+    float* dz = D.dz32;
+
+    float r[RMAX], p[RMAX], sv[RMAX], w[RMAX], dd[RMAX];
+    bool fr[RMAX];
+    int row[RMAX], lbase[RMAX], wr[RMAX];
+    int wmax = 0;
+#pragma unroll
+    for (int k = 0; k < RMAX; ++k) {
+        const int sl = s_beg + warp + PCG_WARPS * k;
+        row[k] = (sl < s_end) ? sl * 32 + lane : -1;
+        lbase[k] = 0;
+        wr[k] = 0;
+        if (sl < s_end) {
+            lbase[k] = (int)(D.slice_off[sl] - S0) + lane;
+            wr[k] = D.slice_w[sl];
+            wmax = wr[k] > wmax ? wr[k] : wmax;
+        }
+        r[k] = p[k] = sv[k] = w[k] = 0.0f;
+        dd[k] = __int_as_float(0x7f800000);
+        fr[k] = false;
+    }
+    // FP64 off-diagonal sums from the streamed FP64 coefficients and vh64
+    auto offdiag64 = [&](double* off) {
+#pragma unroll
+        for (int k = 0; k < RMAX; ++k) off[k] = 0.0;
+        for (int k0 = 0; k0 < wmax; k0 += 4) {
+            double v[RMAX][4];
+#pragma unroll
+            for (int k = 0; k < RMAX; ++k)
+#pragma unroll
+                for (int u = 0; u < 4; ++u)
+                    v[k][u] = (k0 + u < wr[k]) ? __ldcg(D.val + S0 + lbase[k] + 32 * (k0 + u)) : 0.0;
+#pragma unroll
+            for (int k = 0; k < RMAX; ++k)
+#pragma unroll
+                for (int u = 0; u < 4; ++u) {
+                    const double g = (k0 + u < wr[k]) ? vh64[lcs[lbase[k] + 32 * (k0 + u)]] : 0.0;
+                    off[k] = fma(v[k][u], g, off[k]);
+                }
+        }
+    };
+    // FP32 off-diagonal sums from the resident coefficients and a float halo
+    auto offdiag32 = [&](const float* vx, float* off) {
+#pragma unroll
+        for (int k = 0; k < RMAX; ++k) off[k] = 0.0f;
+        for (int kk = 0; kk < wmax; ++kk) {
+#pragma unroll
+            for (int k = 0; k < RMAX; ++k)
+                if (kk < wr[k]) {
+                    const int sl = lbase[k] + 32 * kk;
+                    off[k] = fmaf(val32s[sl], vx[lcs[sl]], off[k]);
+                }
+        }
+    };
+    auto stage64 = [&](const double* x) {
+        __syncthreads();
+        for (int k0 = threadIdx.x; k0 < nh; k0 += 4 * PCG_THREADS) {
+            double a[4];
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                const int k = k0 + u * PCG_THREADS;
+                a[u] = __ldcg(x + (k < nh ? hidx[k] : 0));
+            }
+#pragma unroll
+            for (int u = 0; u < 4; ++u)
+                if (k0 + u * PCG_THREADS < nh) vh64[k0 + u * PCG_THREADS] = a[u];
+        }
+        __syncthreads();
+    };
+    // true residual of the own rows into r[], rb[buf]; returns partials
+    auto true_residual = [&](int buf, Acc6& acc) {
+        stage64(D.pres);
+        double off[RMAX];
+        offdiag64(off);
+#pragma unroll
+        for (int k = 0; k < RMAX; ++k) {
+            const int i = row[k];
+            if (i < 0) continue;
+            const double y = fma(D.pdiag[i], D.pres[i], off[k]);
+            double ri = (D.nflag[i] & 1) ? D.rhs1[i] - y : 0.0;
+            if (!fr[k]) ri = 0.0;
+            if (fr[k]) {
+                if (!isfinite(ri)) acc.flag = fmax(acc.flag, 2.0);
+                acc.c = fma(ri, ri, acc.c);
+                acc.mx = fmax(acc.mx, fabs(ri));
+            }
+            r[k] = (float)ri;
+            rb[buf][i] = r[k];
+            pb[i] = p[k];
+        }
+    };
+    // w = A z and s = A p from the staged halos (p taken as zero when
+    // zero_p, which restarts the direction); partials of r.z, z.w, z.s, p.w
+    // and p.s, from which the step length of the next direction
+    // (z + beta p).A(z + beta p) follows directly
+    auto refresh_ws = [&](int buf, bool zero_p, Acc8& acc) {
+        __syncthreads();
+        for (int k0 = threadIdx.x; k0 < nh; k0 += 4 * PCG_THREADS) {
+            float a[4], c[4];
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                const int k = k0 + u * PCG_THREADS;
+                const int j = k < nh ? hidx[k] : 0;
+                a[u] = __ldcg(rb[buf] + j);
+                c[u] = zero_p ? 0.0f : __ldcg(pb + j);
+            }
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                const int k = k0 + u * PCG_THREADS;
+                if (k < nh) { vz[k] = a[u] / dzh[k]; vp[k] = c[u]; }
+            }
+        }
+        __syncthreads();
+        float offz[RMAX], offp[RMAX];
+        offdiag32(vz, offz);
+        offdiag32(vp, offp);
+#pragma unroll
+        for (int k = 0; k < RMAX; ++k) {
+            const int i = row[k];
+            if (i < 0) continue;
+            if (zero_p) p[k] = 0.0f;
+            const float pd = (float)D.pdiag[i];
+            const float zi = r[k] / dd[k];
+            w[k] = fr[k] ? fmaf(pd, zi, offz[k]) : 0.0f;
+            sv[k] = fr[k] ? fmaf(pd, p[k], offp[k]) : 0.0f;
+            wb[buf][i] = w[k];
+            sb[buf][i] = sv[k];
+            if (fr[k]) {
+                const double zd = zi, pv = p[k];
+                acc.a = fma((double)r[k], zd, acc.a);
+                acc.b = fma(zd, (double)w[k], acc.b);
+                acc.c = fma(zd, (double)sv[k], acc.c);
+                acc.d = fma(pv, (double)w[k], acc.d);
+                acc.e = fma(pv, (double)sv[k], acc.e);
+            }
+        }
+    };
+
+    // ---- phase 0a: FP64 r0 = b - A x0, its norm, dz
+    Acc6 acc{0.0, 0.0, 0.0, 0.0, 0.0};
+#pragma unroll
+    for (int k = 0; k < RMAX; ++k) {
+        const int i = row[k];
+        if (i < 0) continue;
+        const uint8_t f = D.nflag[i];
+        fr[k] = (f & 1) && !(f & 4);
+        const double pd = D.pdiag[i];
+        if (fr[k]) {
+            if (D.precond && !(isfinite(pd) && pd > 1.0e-30)) acc.flag = fmax(acc.flag, 1.0);
+            dd[k] = D.precond ? (float)pd : 1.0f;
+        }
+        dz[i] = dd[k];
+        sb[0][i] = 0.0f;
+    }
+    true_residual(0, acc);
+    Acc6 t{0.0, 0.0, 0.0, 0.0, 0.0};
+    if (!grid_allreduce3(acc, D, phase, t)) return;
+    ++phase;
+    const double init = sqrt(t.c);
+    if (init <= 1.0e-300) { cg_finish(D, 0, 1, init, init, 0.0, t.mx); return; }
+    if (cg_converged(D.conv_test, 1.0, t.mx, D.rel_tol, D.abs_tol)) { cg_finish(D, 0, 1, init, init, 1.0, t.mx); return; }
+    if (t.flag >= 2.0) { if (b == 0 && threadIdx.x == 0) set_status(D.status, 4, ST_PCG, 0, R_PCG_RESID); return; }
+    if (t.flag >= 1.0) { if (b == 0 && threadIdx.x == 0) set_status(D.status, 1, ST_PCG, 0, R_PCG_DIAG); return; }
+    double rr_last = t.c;
+
+    // ---- phase 0b: z0, w0 = A z0 (p = 0, s = 0)
+    __syncthreads();
+    for (int k = threadIdx.x; k < nh; k += PCG_THREADS) dzh[k] = __ldcg(dz + hidx[k]);
+    Acc8 a8{0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+    refresh_ws(0, true, a8);
+    Acc8 t8{0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+    if (!grid_allreduce5(a8, D, phase, t8)) return;
+    ++phase;
+    double gam = t8.a;
+    if (gam <= 1.0e-300 || !isfinite(gam)) { if (b == 0 && threadIdx.x == 0) set_status(D.status, 3, ST_PCG, 0, R_PCG_RZ0); return; }
+    double den = t8.b;
+    double beta = 0.0, fin = init, rel = 1.0, mx = 0.0, alpha = 0.0;
+    int it = 0, conv = 0, outer = 0, last_fix = 0;
+    for (it = 1; it <= D.max_iter; ++it) {
+        if (fabs(den) <= 1.0e-300 || !isfinite(den)) { if (b == 0 && threadIdx.x == 0) set_status(D.status, 3, ST_PCG, it, R_PCG_PAP); return; }
+        alpha = gam / den;
+        const float a32 = (float)alpha, b32 = (float)beta;
+        const int po = (it - 1) & 1, pn = it & 1;
+        __syncthreads();
+        {
+            const float* so = sb[po];
+            const float* wo = wb[po];
+            const float* ro = rb[po];
+            for (int k0 = threadIdx.x; k0 < nh; k0 += 4 * PCG_THREADS) {
+                float a[4], c[4], e[4];
+#pragma unroll
+                for (int u = 0; u < 4; ++u) {
+                    const int k = k0 + u * PCG_THREADS;
+                    const int j = k < nh ? hidx[k] : 0;
+                    a[u] = __ldcg(so + j);
+                    c[u] = __ldcg(wo + j);
+                    e[u] = __ldcg(ro + j);
+                }
+#pragma unroll
+                for (int u = 0; u < 4; ++u) {
+                    const int k = k0 + u * PCG_THREADS;
+                    if (k < nh) {
+                        const float sj = fmaf(b32, a[u], c[u]);
+                        const float rj = fmaf(-a32, sj, e[u]);
+                        vz[k] = rj / dzh[k];
+                    }
+                }
+            }
+        }
+        __syncthreads();
+#pragma unroll
+        for (int k = 0; k < RMAX; ++k) {
+            const int i = row[k];
+            if (i < 0) continue;
+            const float zo = r[k] / dd[k];
+            p[k] = fr[k] ? fmaf(b32, p[k], zo) : 0.0f;
+            sv[k] = fmaf(b32, sv[k], w[k]);
+            if (fr[k]) D.pres[i] = fma(alpha, (double)p[k], D.pres[i]);
+            r[k] = fmaf(-a32, sv[k], r[k]);
+            rb[pn][i] = r[k];
+            sb[pn][i] = sv[k];
+        }
+        float off[RMAX];
+        offdiag32(vz, off);
+        Acc6 a6{0.0, 0.0, 0.0, 0.0, 0.0};
+#pragma unroll
+        for (int k = 0; k < RMAX; ++k) {
+            const int i = row[k];
+            if (i < 0) continue;
+            const float zi = r[k] / dd[k];
+            w[k] = fr[k] ? fmaf((float)D.pdiag[i], zi, off[k]) : 0.0f;
+            wb[pn][i] = w[k];
+            if (fr[k]) {
+                if (!isfinite(r[k])) a6.flag = 1.0;
+                a6.a = fma((double)r[k], (double)zi, a6.a);
+                a6.b = fma((double)zi, (double)w[k], a6.b);
+                a6.c = fma((double)r[k], (double)r[k], a6.c);
+                a6.mx = fmax(a6.mx, fabs((double)r[k]));
+            }
+        }
+        t = Acc6{0.0, 0.0, 0.0, 0.0, 0.0};
+        if (!grid_allreduce3(a6, D, phase, t)) return;
+        ++phase;
+        if (t.flag > 0.0) { if (b == 0 && threadIdx.x == 0) set_status(D.status, 4, ST_PCG, it, R_PCG_RESID); return; }
+        fin = sqrt(t.c);
+        mx = t.mx;
+        rel = fin / init;
+        const bool candidate = cg_converged(D.conv_test, rel, mx, D.rel_tol, D.abs_tol);
+        if (candidate || t.c <= RU_FACTOR * RU_FACTOR * rr_last || it - last_fix >= RU_STALL) {
+            // residual replacement from the FP64 coefficients and pressure
+            Acc6 u1{0.0, 0.0, 0.0, 0.0, 0.0};
+            true_residual(pn, u1);
+            t = Acc6{0.0, 0.0, 0.0, 0.0, 0.0};
+            if (!grid_allreduce3(u1, D, phase, t)) return;
+            ++phase;
+            ++outer;
+            last_fix = it;
+            if (t.flag > 0.0) { if (b == 0 && threadIdx.x == 0) set_status(D.status, 4, ST_PCG, it, R_PCG_RESID); return; }
+            fin = sqrt(t.c);
+            mx = t.mx;
+            rel = fin / init;
+            // no progress of the true residual since the last correction:
+            // the FP32 recurrences have lost the Krylov relations, restart
+            const bool restart = t.c >= rr_last;
+            rr_last = t.c;
+            if (cg_converged(D.conv_test, rel, mx, D.rel_tol, D.abs_tol)) { conv = 1; break; }
+            Acc8 u2{0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+            refresh_ws(pn, restart, u2);
+            t8 = Acc8{0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+            if (!grid_allreduce5(u2, D, phase, t8)) return;
+            ++phase;
+            const double gn = t8.a;
+            if (gn <= 1.0e-300 || !isfinite(gn)) { if (b == 0 && threadIdx.x == 0) set_status(D.status, 3, ST_PCG, it, R_PCG_RZ); return; }
+            // next direction z + beta p with its curvature computed, not recurred
+            beta = restart ? 0.0 : gn / gam;
+            den = t8.b + beta * (t8.c + t8.d) + beta * beta * t8.e;
+            gam = gn;
+            continue;
+        }
+        const double gn = t.a;
+        if (gn <= 1.0e-300 || !isfinite(gn)) { if (b == 0 && threadIdx.x == 0) set_status(D.status, 3, ST_PCG, it, R_PCG_RZ); return; }
+        beta = gn / gam;
+        den = t.b - beta * gn / alpha;
+        gam = gn;
+    }
+    if (it > D.max_iter) it = D.max_iter;
+    cg_finish(D, it, conv, init, fin, rel, mx);
+    if (b == 0 && threadIdx.x == 0) D.out->outer = outer;
+    if (!conv && b == 0 && threadIdx.x == 0) set_status(D.status, 2, ST_PCG, it, R_PCG_MAXIT);
+}
+
 // Self-test of the bounded device wait: CTA 0 leaves without arriving, so the
 // other CTAs' barrier waits can only end by running out of their spin limit.
 __global__ void k_barrier_selftest(unsigned* bar, DevStatus* st)
@@ -1077,6 +1478,15 @@ void PcgEngine::init(const HostModel& m, const uint8_t* nflag, const double* pfi
     ncontrib = static_cast<long long>(P.cent.size());
     nnz_offdiag = 0;
     for (size_t q = 0; q + 1 < P.cptr.size(); ++q) nnz_offdiag += (P.cptr[q + 1] > P.cptr[q]) ? 1 : 0;
+    NP = nslices * 32;
+    d_row_node = dalloc<int>(P.row_node.size());
+    CUDA_OK(cudaMemcpy(d_row_node, P.row_node.data(), P.row_node.size() * sizeof(int), cudaMemcpyHostToDevice));
+    // columns as row positions: the solver works in row-position order
+    std::vector<int> pos_of(static_cast<size_t>(N), 0);
+    for (size_t p = 0; p < P.row_node.size(); ++p)
+        if (P.row_node[p] >= 0) pos_of[static_cast<size_t>(P.row_node[p])] = static_cast<int>(p);
+    std::vector<int> colp(static_cast<size_t>(nslots));
+    for (size_t t = 0; t < colp.size(); ++t) colp[t] = pos_of[static_cast<size_t>(P.col[t])];
     d_slice_off = dalloc<long long>(P.slice_off.size());
     d_slice_w = dalloc<int>(P.slice_w.size());
     d_col = dalloc<int>(static_cast<size_t>(nslots));
@@ -1085,18 +1495,20 @@ void PcgEngine::init(const HostModel& m, const uint8_t* nflag, const double* pfi
     d_val = dalloc<double>(static_cast<size_t>(nslots));
     CUDA_OK(cudaMemcpy(d_slice_off, P.slice_off.data(), P.slice_off.size() * sizeof(long long), cudaMemcpyHostToDevice));
     CUDA_OK(cudaMemcpy(d_slice_w, P.slice_w.data(), P.slice_w.size() * sizeof(int), cudaMemcpyHostToDevice));
-    if (nslots) CUDA_OK(cudaMemcpy(d_col, P.col.data(), static_cast<size_t>(nslots) * sizeof(int), cudaMemcpyHostToDevice));
+    if (nslots) CUDA_OK(cudaMemcpy(d_col, colp.data(), static_cast<size_t>(nslots) * sizeof(int), cudaMemcpyHostToDevice));
     CUDA_OK(cudaMemcpy(d_cptr, P.cptr.data(), P.cptr.size() * sizeof(long long), cudaMemcpyHostToDevice));
     if (ncontrib) CUDA_OK(cudaMemcpy(d_cent, P.cent.data(), static_cast<size_t>(ncontrib) * sizeof(int), cudaMemcpyHostToDevice));
     CUDA_OK(cudaMemset(d_val, 0, static_cast<size_t>(nslots ? nslots : 1) * sizeof(double)));
-    const size_t n = static_cast<size_t>(N);
+    const size_t n = static_cast<size_t>(NP);
     d_r = dalloc<double>(2 * n); d_z = dalloc<double>(n); d_pA = dalloc<double>(n);
     d_pB = dalloc<double>(n); d_q = dalloc<double>(2 * n);
+    d_xp = dalloc<double>(n); d_bp = dalloc<double>(n); d_dp = dalloc<double>(n);
+    d_fp = dalloc<uint8_t>(n);
     CUDA_OK(cudaMemset(d_pB, 0, n * sizeof(double)));
     if (mixed) {
         d_val32 = dalloc<float>(static_cast<size_t>(nslots));
-        d_f32 = dalloc<float>(7 * n);
-        CUDA_OK(cudaMemset(d_f32, 0, 7 * n * sizeof(float)));
+        d_f32 = dalloc<float>(8 * n);
+        CUDA_OK(cudaMemset(d_f32, 0, 8 * n * sizeof(float)));
     }
     d_nflag = nflag;
     d_pfix = pfix;
@@ -1144,13 +1556,13 @@ void PcgEngine::init(const HostModel& m, const uint8_t* nflag, const double* pfi
                 const int sb = static_cast<int>(static_cast<long long>(bb) * nslices / g);
                 const int se = static_cast<int>(static_cast<long long>(bb + 1) * nslices / g);
                 const long long a0 = P.slice_off[static_cast<size_t>(sb)], a1 = P.slice_off[static_cast<size_t>(se)];
-                cols.assign(P.col.begin() + a0, P.col.begin() + a1);
+                cols.assign(colp.begin() + a0, colp.begin() + a1);
                 std::sort(cols.begin(), cols.end());
                 cols.erase(std::unique(cols.begin(), cols.end()), cols.end());
                 if (cols.size() > 65535) { fits = false; break; }
                 for (long long t = a0; t < a1; ++t)
                     lcol[static_cast<size_t>(t)] = static_cast<unsigned short>(
-                        std::lower_bound(cols.begin(), cols.end(), P.col[static_cast<size_t>(t)]) - cols.begin());
+                        std::lower_bound(cols.begin(), cols.end(), colp[static_cast<size_t>(t)]) - cols.begin());
                 hidx.insert(hidx.end(), cols.begin(), cols.end());
                 hptr[static_cast<size_t>(bb) + 1] = static_cast<int>(hidx.size());
                 hmax = std::max(hmax, static_cast<int>(cols.size()));
@@ -1173,6 +1585,21 @@ void PcgEngine::init(const HostModel& m, const uint8_t* nflag, const double* pfi
             CUDA_OK(cudaMemcpy(d_halo_idx, hidx.data(), hidx.size() * sizeof(int), cudaMemcpyHostToDevice));
             if (!lcol.empty()) CUDA_OK(cudaMemcpy(d_lcol, lcol.data(), lcol.size() * sizeof(unsigned short), cudaMemcpyHostToDevice));
             dev_halo_max = hmax;
+            dev_slot_max = static_cast<int>(smax);
+            if (mixed && want == 4) {
+                const void* mc[4] = {reinterpret_cast<const void*>(k_pcg32m<1>), reinterpret_cast<const void*>(k_pcg32m<2>),
+                                     reinterpret_cast<const void*>(k_pcg32m<4>), reinterpret_cast<const void*>(k_pcg32m<8>)};
+                const size_t ms = static_cast<size_t>(hmax) * 16 + static_cast<size_t>(smax) * 6 + 16;
+                int per = 0;
+                if (ms <= 220 * 1024 &&
+                    cudaFuncSetAttribute(mc[c], cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(ms)) == cudaSuccess &&
+                    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, mc[c], PCG_THREADS, ms) == cudaSuccess &&
+                    per * sms >= g) {
+                    mixed_ok = true;
+                    mixed_smem = ms;
+                }
+                cudaGetLastError();
+            }
         }
     }
     if (variant == 1 && kernel_choice != 1) {
@@ -1190,28 +1617,32 @@ void PcgEngine::init(const HostModel& m, const uint8_t* nflag, const double* pfi
     CUDA_OK(cudaMemset(d_bar, 0, 4 * sizeof(unsigned)));
 
     dev = PcgDev{};
-    dev.N = N; dev.E = E; dev.nslices = nslices; dev.nblocks = nblocks;
+    dev.N = NP; dev.NN = N; dev.E = E; dev.nslices = nslices; dev.nblocks = nblocks;
     dev.slice_off = d_slice_off; dev.slice_w = d_slice_w; dev.col = d_col; dev.val = d_val;
     dev.val32 = d_val32; dev.cptr = d_cptr; dev.cent = d_cent;
     dev.nflag = d_nflag; dev.pfix = d_pfix;
     dev.r = d_r; dev.z = d_z; dev.pA = d_pA; dev.pB = d_pB; dev.q = d_q;
     if (mixed) {
-        dev.r32 = d_f32; dev.z32 = d_f32 + n; dev.pA32 = d_f32 + 2 * n; dev.pB32 = d_f32 + 3 * n;
-        dev.q32 = d_f32 + 4 * n; dev.x32 = d_f32 + 5 * n; dev.dinv32 = d_f32 + 6 * n;
+        dev.r32 = d_f32; dev.w32 = d_f32 + 2 * n; dev.s32 = d_f32 + 4 * n;
+        dev.p32 = d_f32 + 6 * n; dev.dz32 = d_f32 + 7 * n;
     }
+    dev.slot_max = dev_slot_max;
     dev.part = d_part; dev.bar = d_bar; dev.status = d_status; dev.out = d_out;
     dev.halo_ptr = d_halo_ptr; dev.halo_idx = d_halo_idx; dev.lcol = d_lcol; dev.halo_max = dev_halo_max;
+    dev.row_node = d_row_node;
 }
 
 void PcgEngine::release()
 {
     void* ptrs[] = {d_slice_off, d_slice_w, d_col, d_cptr, d_cent, d_val, d_val32, d_r, d_z, d_pA,
-                    d_pB, d_q, d_f32, d_part, d_bar, d_out, d_halo_ptr, d_halo_idx, d_lcol};
+                    d_pB, d_q, d_f32, d_part, d_bar, d_out, d_halo_ptr, d_halo_idx, d_lcol, d_row_node,
+                    d_xp, d_bp, d_dp, d_fp};
     for (void* p : ptrs) if (p) cudaFree(p);
     d_slice_off = nullptr; d_slice_w = nullptr; d_col = nullptr; d_cptr = nullptr; d_cent = nullptr;
     d_val = nullptr; d_val32 = nullptr; d_r = d_z = d_pA = d_pB = d_q = nullptr; d_f32 = nullptr;
     d_part = nullptr; d_bar = nullptr; d_out = nullptr;
-    d_halo_ptr = nullptr; d_halo_idx = nullptr; d_lcol = nullptr;
+    d_halo_ptr = nullptr; d_halo_idx = nullptr; d_lcol = nullptr; d_row_node = nullptr;
+    d_xp = d_bp = d_dp = nullptr; d_fp = nullptr;
 }
 
 void PcgEngine::assemble_from_state(const DevState& S, cudaStream_t st)
@@ -1232,7 +1663,7 @@ void PcgEngine::multiply(const double* pdiag, const double* x, double* y, cudaSt
 {
     PcgDev D = dev;
     D.pdiag = const_cast<double*>(pdiag);
-    k_ell_multiply<<<(N + 255) / 256, 256, 0, st>>>(D, x, y);
+    k_ell_multiply<<<(nslices * 32 + 255) / 256, 256, 0, st>>>(D, x, y);
 }
 
 cbs3d_status PcgEngine::solve(double* pres, double* rhs1, double* pdiag, int precond, int conv_test,
@@ -1244,7 +1675,10 @@ cbs3d_status PcgEngine::solve(double* pres, double* rhs1, double* pdiag, int pre
     D.precond = precond; D.conv_test = conv_test; D.max_iter = max_iter;
     D.rel_tol = rel_tol; D.abs_tol = abs_tol; D.inner_tol = inner_tol;
     k_impose<<<(N + 255) / 256, 256, 0, st>>>(D);
+    k_perm_in<<<(NP + 255) / 256, 256, 0, st>>>(D, pres, rhs1, pdiag, D.nflag, d_xp, d_bp, d_dp, d_fp);
+    D.pres = d_xp; D.rhs1 = d_bp; D.pdiag = d_dp; D.nflag = d_fp;
     CUDA_OK(cudaMemsetAsync(d_bar, 0, 2 * sizeof(unsigned), st));
+    CUDA_OK(cudaMemsetAsync(d_out, 0, sizeof(CgOut), st));
     void* args[] = {&D};
     const void* fn = reinterpret_cast<const void*>(k_pcg64);
     size_t smem = 0;
@@ -1259,6 +1693,12 @@ cbs3d_status PcgEngine::solve(double* pres, double* rhs1, double* pdiag, int pre
         else if (rmax == 4) fn = reinterpret_cast<const void*>(k_pcg64h<4>);
         else fn = reinterpret_cast<const void*>(k_pcg64h<8>);
         smem = halo_smem;
+    } else if (variant == 4 && mixed_ok) {
+        if (rmax == 1) fn = reinterpret_cast<const void*>(k_pcg32m<1>);
+        else if (rmax == 2) fn = reinterpret_cast<const void*>(k_pcg32m<2>);
+        else if (rmax == 4) fn = reinterpret_cast<const void*>(k_pcg32m<4>);
+        else fn = reinterpret_cast<const void*>(k_pcg32m<8>);
+        smem = mixed_smem;
     } else if (variant == 4) {
         if (rmax == 1) fn = reinterpret_cast<const void*>(k_pcg64c<1>);
         else if (rmax == 2) fn = reinterpret_cast<const void*>(k_pcg64c<2>);
@@ -1269,6 +1709,7 @@ cbs3d_status PcgEngine::solve(double* pres, double* rhs1, double* pdiag, int pre
     if (ev0) CUDA_OK(cudaEventRecord(ev0, st));
     CUDA_OK(cudaLaunchCooperativeKernel(fn, dim3(nblocks), dim3(PCG_THREADS), args, smem, st));
     if (ev1) CUDA_OK(cudaEventRecord(ev1, st));
+    k_perm_out<<<(NP + 255) / 256, 256, 0, st>>>(D, d_xp, pres);
     if (sync) CUDA_OK(cudaStreamSynchronize(st));
     return CBS3D_OK;
 }
@@ -1292,6 +1733,12 @@ cbs3d_status PcgEngine::read_result(cbs3d_cg_result& r, cudaStream_t st)
 
 size_t PcgEngine::bytes_per_iter() const
 {
+    if (variant == 4 && mixed_ok) {
+        // coefficients resident in shared memory; per node: r, w, s of the
+        // previous iteration read once for staging (12), r, s, w written (12),
+        // pressure read and written (16), pdiag read (8)
+        return static_cast<size_t>(N) * 48;
+    }
     if (variant == 4) {
         // coefficient per pair entry; per node: r, w, s of the previous
         // iteration read once for staging (24), r, s, w written (24), pressure

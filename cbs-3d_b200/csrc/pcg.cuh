@@ -20,10 +20,13 @@ struct CgOut {
 };
 
 struct PcgDev {
-    int N, E, nslices;
+    int N;                       // row positions (nslices*32); the solver's vectors use this order
+    int NN;                      // nodes (the caller's arrays)
+    int E, nslices;
     int nblocks;
     int precond, conv_test, max_iter;
     double rel_tol, abs_tol, inner_tol;
+    const int* row_node;         // nslices*32: node of each row position (-1 padding)
     const long long* slice_off;
     const int* slice_w;
     const int* col;
@@ -31,11 +34,13 @@ struct PcgDev {
     float* val32;
     const long long* cptr;
     const int* cent;
-    const uint8_t* nflag;        // bit0 pressure-active (touches fluid), bit2 fixed
+    const uint8_t* nflag;        // bit0 pressure-active (touches fluid), bit2 fixed (position order in kernels)
     const double* pfix;
     double *pres, *rhs1, *pdiag;
     double *r, *z, *pA, *pB, *q;
-    float *r32, *z32, *pA32, *pB32, *q32, *x32, *dinv32;
+    float *r32, *w32, *s32;      // mixed: 2N each (parity buffers)
+    float *p32, *dz32;           // mixed: N each
+    int slot_max;                // largest CTA slot range (shared-memory sizing)
     const int* halo_ptr;         // nblocks+1: each CTA's halo node list in halo_idx
     const int* halo_idx;
     const unsigned short* lcol;  // per slot: column as an index into its CTA's halo
@@ -63,7 +68,8 @@ public:
     cbs3d_status solve(double* d_pres, double* d_rhs1, double* d_pdiag, int precond, int conv_test,
                        int max_iter, double rel_tol, double abs_tol, cudaStream_t st, bool sync,
                        cudaEvent_t ev0 = nullptr, cudaEvent_t ev1 = nullptr);
-    int extra_launches_per_solve() const { return 0; }
+    // impose, permute in, solver, permute out
+    int launches_per_solve() const { return 4; }
     cbs3d_status read_result(cbs3d_cg_result& r, cudaStream_t st);
     // y = A x with the assembled operator (identity rows on fixed nodes).
     void multiply(const double* d_pdiag, const double* d_x, double* d_y, cudaStream_t st);
@@ -72,11 +78,17 @@ public:
     int rmax = 0;            // rows per thread of the register-resident kernels (0: global kernel)
     int variant = 1;         // 1 global vectors, 2 register rows, 3 + shared-memory halo, 4 + one sync per iteration
     size_t halo_smem = 0;    // dynamic shared memory of the halo kernel
+    size_t mixed_smem = 0;   // dynamic shared memory of the mixed-precision kernel
+    bool mixed_ok = false;   // mixed precision runs on the FP32 kernel (else FP64)
+    int dev_slot_max = 0;
     int *d_halo_ptr = nullptr, *d_halo_idx = nullptr;
     unsigned short* d_lcol = nullptr;
+    int* d_row_node = nullptr;
+    double *d_xp = nullptr, *d_bp = nullptr, *d_dp = nullptr;   // pressure, rhs, diagonal by position
+    uint8_t* d_fp = nullptr;
     int dev_halo_max = 0;
     double inner_tol = 1.0e-5;
-    int N = 0, E = 0, nslices = 0, nblocks = 0;
+    int N = 0, NP = 0, E = 0, nslices = 0, nblocks = 0;
     long long nslots = 0, ncontrib = 0;
     long long *d_slice_off = nullptr, *d_cptr = nullptr;
     int *d_slice_w = nullptr, *d_col = nullptr, *d_cent = nullptr;

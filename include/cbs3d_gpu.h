@@ -126,7 +126,10 @@ typedef struct cbs3d_step_stats {
     double pcg_seconds;      /* with time_pcg: summed duration of the PCG kernel launches */
     int pcg_launches;        /* with time_pcg: PCG kernel launches timed */
     long long kernel_launches; /* kernels this library launched during the call */
-    double pcg_bytes_per_iter; /* algorithmic bytes of one PCG iteration (see PCG roofline) */
+    double pcg_bytes_per_iter; /* bytes one PCG iteration of the selected kernel moves */
+    int pcg_kernel;          /* PCG kernel in use: 1 global vectors, 2 register rows,
+                                3 shared-memory halo, 4 single-reduction (CG-CG),
+                                5 mixed FP32/FP64 */
 } cbs3d_step_stats;
 
 typedef struct cbs3d_ctx cbs3d_ctx;

@@ -192,3 +192,37 @@ def test_pcg_variants_bitwise_identical(name):
     for other in runs[1:]:
         for x, y in zip(runs[0], other):
             assert bitwise(x, y)
+
+
+MIXED_TOL = 1e-8     # FP32 inner PCG with FP64 defect correction, vs FP64
+
+
+@pytest.mark.parametrize("name", ["cav6j", "chan_sym", "cht"])
+def test_mixed_precision_vs_reference(name):
+    """Mixed mode (extension, no reference counterpart): every solve stops
+    on the FP64 true residual meeting relToler, so short runs agree with the
+    reference's FP64 golden vectors to MIXED_TOL."""
+    gpu = _gpu()
+    c, _, z = _ctx(name, precision=gpu.MIXED)
+    st = c.step(int(z["nsteps"][0]))
+    u, p, t = c.fields()
+    assert st.cg.outer_sweeps >= 1
+    assert rel_l2(u, z["ref_final_unkno"]) <= MIXED_TOL
+    assert rel_l2(p, z["ref_final_pres"]) <= MIXED_TOL
+    if _param(z, "temp_calc") or _param(z, "material_enabled"):
+        assert rel_l2(t, z["ref_final_temperature"]) <= MIXED_TOL
+
+
+def test_mixed_precision_vs_fp64_jittered_cavity():
+    """The benchmark's case family (jittered cavity, Re=400) at 24^3: mixed
+    and FP64 engines agree to MIXED_TOL on u and p after 8 steps."""
+    from cbs3d import cases
+    gpu = _gpu()
+    case = cases.cavity(24, re=400.0, ntime=10 ** 6, jitter=0.15, seed=1234)
+    a = gpu.Context(case)
+    a.step(8)
+    b = gpu.Context(case, precision=gpu.MIXED)
+    b.step(8)
+    (ua, pa, _), (ub, pb, _) = a.fields(), b.fields()
+    assert rel_l2(ub, ua) <= MIXED_TOL
+    assert rel_l2(pb, pa) <= MIXED_TOL
