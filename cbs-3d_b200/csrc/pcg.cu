@@ -136,85 +136,15 @@ struct Acc4 {
 };
 
 // Grid-wide all-reduce of (sum a, sum b, max mx, max flag) fused with the
-// grid barrier.  Each CTA stores its partial and arrives on a counter
-// (release); the CTA that arrives last reduces all partials in a fixed tree
-// -- the same tree whichever CTA it is, so the totals are deterministic --
-// publishes them and bumps the generation (release).  The others wait for the
-// generation (acquire, bounded by the spin limit of grid_barrier) and read the
-// totals.  One partial read per CTA instead of every CTA reading all partials.
+// grid barrier (grid_allreduce_v below).
+template <int NV, int NSUM>
+__device__ __forceinline__ bool grid_allreduce_v(double (&v)[NV], const PcgDev& D, int phase, double (&out)[NV]);
+
 __device__ __forceinline__ bool grid_allreduce(Acc4 v, const PcgDev& D, int phase, Acc4& out)
 {
-    __shared__ double sm[PCG_WARPS][4];
-    __shared__ double tot[4];
-    __shared__ int s_last, s_ok;
-    const int G = gridDim.x;
-    for (int o = 16; o > 0; o >>= 1) {
-        v.a += __shfl_down_sync(0xffffffffu, v.a, o);
-        v.b += __shfl_down_sync(0xffffffffu, v.b, o);
-        v.mx = fmax(v.mx, __shfl_down_sync(0xffffffffu, v.mx, o));
-        v.flag = fmax(v.flag, __shfl_down_sync(0xffffffffu, v.flag, o));
-    }
-    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    if (lane == 0) { sm[w][0] = v.a; sm[w][1] = v.b; sm[w][2] = v.mx; sm[w][3] = v.flag; }
-    __syncthreads();
-    unsigned* cnt = D.bar;
-    unsigned* gen = D.bar + 1;
-    double* totals = D.part + (size_t)G * 4 + (size_t)(phase & 1) * 4;
-    if (threadIdx.x == 0) {
-        double a = 0.0, b = 0.0, mx = 0.0, fl = 0.0;
-        for (int k = 0; k < PCG_WARPS; ++k) { a += sm[k][0]; b += sm[k][1]; mx = fmax(mx, sm[k][2]); fl = fmax(fl, sm[k][3]); }
-        double* p = D.part + (size_t)blockIdx.x * 4;
-        __stcg(p, a); __stcg(p + 1, b); __stcg(p + 2, mx); __stcg(p + 3, fl);
-        const unsigned g = ld_acquire(gen);
-        unsigned arrived;
-        asm volatile("atom.add.acq_rel.gpu.global.u32 %0, [%1], 1;" : "=r"(arrived) : "l"(cnt) : "memory");
-        s_last = (arrived == (unsigned)G - 1) ? 1 : 0;
-        s_ok = 1;
-        if (!s_last) {
-            const long long t0 = clock64();
-            while (ld_acquire(gen) == g) {
-                if (ld_relaxed_int(&D.status->code) != 0) { s_ok = 0; break; }
-                if (clock64() - t0 > (1LL << 31)) {
-                    set_status(D.status, 5 /*CBS3D_TIMEOUT*/, ST_PCG, 0, R_PCG_BARRIER);
-                    s_ok = 0;
-                    break;
-                }
-                __nanosleep(20);
-            }
-            if (s_ok) { tot[0] = __ldcg(totals); tot[1] = __ldcg(totals + 1); tot[2] = __ldcg(totals + 2); tot[3] = __ldcg(totals + 3); }
-        }
-    }
-    __syncthreads();
-    if (s_last) {
-        // fixed tree over the G partials: thread t takes t, t+T, ...; then warps; then thread 0
-        double a = 0.0, b = 0.0, mx = 0.0, fl = 0.0;
-        for (int k = threadIdx.x; k < G; k += PCG_THREADS) {
-            const double* p = D.part + (size_t)k * 4;
-            a += __ldcg(p); b += __ldcg(p + 1); mx = fmax(mx, __ldcg(p + 2)); fl = fmax(fl, __ldcg(p + 3));
-        }
-        for (int o = 16; o > 0; o >>= 1) {
-            a += __shfl_down_sync(0xffffffffu, a, o);
-            b += __shfl_down_sync(0xffffffffu, b, o);
-            mx = fmax(mx, __shfl_down_sync(0xffffffffu, mx, o));
-            fl = fmax(fl, __shfl_down_sync(0xffffffffu, fl, o));
-        }
-        __syncthreads();
-        if (lane == 0) { sm[w][0] = a; sm[w][1] = b; sm[w][2] = mx; sm[w][3] = fl; }
-        __syncthreads();
-        if (threadIdx.x == 0) {
-            double ta = 0.0, tb = 0.0, tm = 0.0, tf = 0.0;
-            for (int k = 0; k < PCG_WARPS; ++k) { ta += sm[k][0]; tb += sm[k][1]; tm = fmax(tm, sm[k][2]); tf = fmax(tf, sm[k][3]); }
-            tot[0] = ta; tot[1] = tb; tot[2] = tm; tot[3] = tf;
-            __stcg(totals, ta); __stcg(totals + 1, tb); __stcg(totals + 2, tm); __stcg(totals + 3, tf);
-            atomicExch(cnt, 0u);
-            asm volatile("red.release.gpu.global.add.u32 [%0], 1;" :: "l"(gen) : "memory");
-            if (ld_relaxed_int(&D.status->code) != 0) s_ok = 0;
-        }
-    }
-    __syncthreads();
-    out = Acc4{tot[0], tot[1], tot[2], tot[3]};
-    const bool ok = s_ok != 0;
-    __syncthreads();
+    double a[4] = {v.a, v.b, v.mx, v.flag}, o[4];
+    const bool ok = grid_allreduce_v<4, 2>(a, D, phase, o);
+    out = Acc4{o[0], o[1], o[2], o[3]};
     return ok;
 }
 
@@ -733,16 +663,20 @@ struct Acc6 {
 };
 
 // Grid-wide all-reduce of NV values per thread: the first NSUM summed, the
-// rest max-reduced.  Fixed reduction tree (warp shuffles, warps in order,
-// CTAs by index in the last-arriving CTA), so the result is deterministic.
-// Returns false when the barrier gave up or another CTA raised a status.
+// rest max-reduced.  Every CTA publishes its partials (double-buffered by
+// phase parity), arrives on a 64-bit counter that only grows, waits until
+// all G CTAs of this phase have arrived, and then reduces the G partials
+// itself in a fixed order (thread t takes CTAs t, t+T, ...; warp shuffles;
+// warps in order).  Every CTA therefore computes bit-identical totals without
+// a second round trip through a last-arriving CTA.  The caller passes the
+// number of all-reduces this launch has completed as `phase`.  Returns false
+// when the wait gave up (status TIMEOUT) or another CTA raised a status.
 template <int NV, int NSUM>
 __device__ __forceinline__ bool grid_allreduce_v(double (&v)[NV], const PcgDev& D, int phase, double (&out)[NV])
 {
     static_assert(NV <= 8, "partials hold 8 doubles per CTA");
     __shared__ double sm[PCG_WARPS][NV];
-    __shared__ double tot[NV];
-    __shared__ int s_last, s_ok;
+    __shared__ int s_ok;
     const int G = gridDim.x;
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1)
@@ -756,9 +690,8 @@ __device__ __forceinline__ bool grid_allreduce_v(double (&v)[NV], const PcgDev& 
 #pragma unroll
         for (int q = 0; q < NV; ++q) sm[w][q] = v[q];
     __syncthreads();
-    unsigned* cnt = D.bar;
-    unsigned* gen = D.bar + 1;
-    double* totals = D.part + (size_t)G * 8 + (size_t)(phase & 1) * 8;
+    unsigned long long* cnt = reinterpret_cast<unsigned long long*>(D.bar);
+    double* part = D.part + (size_t)(phase & 1) * G * 8;
     if (threadIdx.x == 0) {
         double t[NV];
 #pragma unroll
@@ -766,70 +699,59 @@ __device__ __forceinline__ bool grid_allreduce_v(double (&v)[NV], const PcgDev& 
         for (int k = 0; k < PCG_WARPS; ++k)
 #pragma unroll
             for (int q = 0; q < NV; ++q) t[q] = q < NSUM ? t[q] + sm[k][q] : fmax(t[q], sm[k][q]);
-        double* p = D.part + (size_t)blockIdx.x * 8;
+        double* p = part + (size_t)blockIdx.x * 8;
 #pragma unroll
         for (int q = 0; q < NV; ++q) __stcg(p + q, t[q]);
-        const unsigned g = ld_acquire(gen);
-        unsigned arrived;
-        asm volatile("atom.add.acq_rel.gpu.global.u32 %0, [%1], 1;" : "=r"(arrived) : "l"(cnt) : "memory");
-        s_last = (arrived == (unsigned)G - 1) ? 1 : 0;
-        s_ok = 1;
-        if (!s_last) {
+        const unsigned long long target = (unsigned long long)(phase + 1) * (unsigned long long)G;
+        unsigned long long arrived;
+        asm volatile("atom.add.acq_rel.gpu.global.u64 %0, [%1], 1;" : "=l"(arrived) : "l"(cnt) : "memory");
+        int ok = 1;
+        if (arrived + 1 < target) {
             const long long t0 = clock64();
-            while (ld_acquire(gen) == g) {
-                if (ld_relaxed_int(&D.status->code) != 0) { s_ok = 0; break; }
+            for (;;) {
+                unsigned long long c;
+                asm volatile("ld.acquire.gpu.global.u64 %0, [%1];" : "=l"(c) : "l"(cnt) : "memory");
+                if (c >= target) break;
+                if (ld_relaxed_int(&D.status->code) != 0) { ok = 0; break; }
                 if (clock64() - t0 > (1LL << 31)) {
                     set_status(D.status, 5 /*CBS3D_TIMEOUT*/, ST_PCG, 0, R_PCG_BARRIER);
-                    s_ok = 0;
+                    ok = 0;
                     break;
                 }
-                __nanosleep(20);
             }
-            if (s_ok)
-#pragma unroll
-                for (int q = 0; q < NV; ++q) tot[q] = __ldcg(totals + q);
         }
+        if (ok && ld_relaxed_int(&D.status->code) != 0) ok = 0;
+        s_ok = ok;
     }
     __syncthreads();
-    if (s_last) {
-        double t[NV];
+    const bool ok = s_ok != 0;
+    double t[NV];
 #pragma unroll
-        for (int q = 0; q < NV; ++q) t[q] = 0.0;
+    for (int q = 0; q < NV; ++q) t[q] = 0.0;
+    if (ok) {
         for (int k = threadIdx.x; k < G; k += PCG_THREADS) {
-            const double* p = D.part + (size_t)k * 8;
+            const double* p = part + (size_t)k * 8;
 #pragma unroll
             for (int q = 0; q < NV; ++q) t[q] = q < NSUM ? t[q] + __ldcg(p + q) : fmax(t[q], __ldcg(p + q));
         }
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1)
-#pragma unroll
-            for (int q = 0; q < NV; ++q) {
-                const double x = __shfl_down_sync(0xffffffffu, t[q], o);
-                t[q] = q < NSUM ? t[q] + x : fmax(t[q], x);
-            }
-        __syncthreads();
-        if (lane == 0)
-#pragma unroll
-            for (int q = 0; q < NV; ++q) sm[w][q] = t[q];
-        __syncthreads();
-        if (threadIdx.x == 0) {
-            double u[NV];
-#pragma unroll
-            for (int q = 0; q < NV; ++q) u[q] = 0.0;
-            for (int k = 0; k < PCG_WARPS; ++k)
-#pragma unroll
-                for (int q = 0; q < NV; ++q) u[q] = q < NSUM ? u[q] + sm[k][q] : fmax(u[q], sm[k][q]);
-#pragma unroll
-            for (int q = 0; q < NV; ++q) { tot[q] = u[q]; __stcg(totals + q, u[q]); }
-            atomicExch(cnt, 0u);
-            asm volatile("red.release.gpu.global.add.u32 [%0], 1;" :: "l"(gen) : "memory");
-            if (ld_relaxed_int(&D.status->code) != 0) s_ok = 0;
-        }
     }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1)
+#pragma unroll
+        for (int q = 0; q < NV; ++q) {
+            const double x = __shfl_down_sync(0xffffffffu, t[q], o);
+            t[q] = q < NSUM ? t[q] + x : fmax(t[q], x);
+        }
+    __syncthreads();
+    if (lane == 0)
+#pragma unroll
+        for (int q = 0; q < NV; ++q) sm[w][q] = t[q];
     __syncthreads();
 #pragma unroll
-    for (int q = 0; q < NV; ++q) out[q] = tot[q];
-    const bool ok = s_ok != 0;
+    for (int q = 0; q < NV; ++q) out[q] = 0.0;
+    for (int k = 0; k < PCG_WARPS; ++k)
+#pragma unroll
+        for (int q = 0; q < NV; ++q) out[q] = q < NSUM ? out[q] + sm[k][q] : fmax(out[q], sm[k][q]);
     __syncthreads();
     return ok;
 }
@@ -1611,7 +1533,7 @@ void PcgEngine::init(const HostModel& m, const uint8_t* nflag, const double* pfi
             if ((per_cta + PCG_WARPS - 1) / PCG_WARPS <= rm[c]) { rmax = rm[c]; nblocks = g; variant = 2; break; }
         }
     }
-    d_part = dalloc<double>(static_cast<size_t>(nblocks) * 8 + 16);
+    d_part = dalloc<double>(static_cast<size_t>(nblocks) * 16);
     d_bar = dalloc<unsigned>(4);
     d_out = dalloc<CgOut>(1);
     CUDA_OK(cudaMemset(d_bar, 0, 4 * sizeof(unsigned)));
@@ -1677,7 +1599,7 @@ cbs3d_status PcgEngine::solve(double* pres, double* rhs1, double* pdiag, int pre
     k_impose<<<(N + 255) / 256, 256, 0, st>>>(D);
     k_perm_in<<<(NP + 255) / 256, 256, 0, st>>>(D, pres, rhs1, pdiag, D.nflag, d_xp, d_bp, d_dp, d_fp);
     D.pres = d_xp; D.rhs1 = d_bp; D.pdiag = d_dp; D.nflag = d_fp;
-    CUDA_OK(cudaMemsetAsync(d_bar, 0, 2 * sizeof(unsigned), st));
+    CUDA_OK(cudaMemsetAsync(d_bar, 0, 4 * sizeof(unsigned), st));
     CUDA_OK(cudaMemsetAsync(d_out, 0, sizeof(CgOut), st));
     void* args[] = {&D};
     const void* fn = reinterpret_cast<const void*>(k_pcg64);
