@@ -286,6 +286,18 @@ def cavity(n: int, re: float = 100.0, ntime: int = 10, jitter: float = 0.0,
     return Case(mesh=m, bc_map=dict(CAVITY_BC), params=p)
 
 
+def cavity_batch(count: int = 48, n_lo: int = 10, n_hi: int = 40, re_lo: float = 50.0, re_hi: float = 1000.0,
+                 seed: int = 2024, ntime: int = 100, rel_tol: float = 1.0e-8, **over) -> list:
+    """Independent lid-driven cavities of uneven size for the batched step:
+    hexes per side uniform in {n_lo..n_hi}, Re log-uniform in [re_lo, re_hi]
+    (nu = 1/Re, lid speed 1), each pressure solve to rel_tol, all from one
+    seed.  Returns the cases; their sizes and Re are in .mesh and .params."""
+    rng = np.random.default_rng(seed)
+    ns = rng.integers(n_lo, n_hi + 1, size=count)
+    res = np.exp(rng.uniform(np.log(re_lo), np.log(re_hi), size=count))
+    return [cavity(int(n), re=float(r), ntime=ntime, relToler=rel_tol, **over) for n, r in zip(ns, res)]
+
+
 def channel(nx: int = 96, ny: int = 16, nz: int = 16, length: float = 6.0, re: float = 100.0,
             ntime: int = 10, symmetry_z: bool = False, **over) -> Case:
     """Channel [0,L]x[0,1]x[0,1]: BC 508 parabolic inlet at x=0, BC 520 outlet

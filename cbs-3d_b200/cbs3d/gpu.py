@@ -101,6 +101,16 @@ class StepStats(ctypes.Structure):
                 ("pcg_kernel", _i)]
 
 
+class BatchOptions(ctypes.Structure):
+    _fields_ = [("base", Options), ("autotune", _i), ("rows_per_thread", _i), ("spread", _i)]
+
+
+class BatchInfo(ctypes.Structure):
+    _fields_ = [("instances", _i), ("waves", _i), ("rows_per_thread", _i), ("spread", _i), ("mixed_waves", _i),
+                ("tuned", _i), ("candidates", _i), ("cand_rows", _i * 8), ("cand_spread", _i * 8),
+                ("cand_ms", _d * 8)]
+
+
 # case-generator parameter names -> cbs3d_params fields
 _PAR_MAP = {
     "l2v": "l2norm_vel_tolerance", "l2T": "l2norm_temp_tolerance", "paraview": "paraview_output",
@@ -149,11 +159,21 @@ def lib():
         L.cbs3d_pcg_destroy.argtypes = [vp]
         L.cbs3d_pcg_last_error.argtypes = [vp]
         L.cbs3d_pcg_last_error.restype = cp
+        L.cbs3d_default_batch_options.argtypes = [ctypes.POINTER(BatchOptions)]
+        L.cbs3d_batch_create.argtypes = [_i, ctypes.POINTER(Mesh), ctypes.POINTER(Params),
+                                         ctypes.POINTER(BatchOptions), ctypes.POINTER(vp), cp, ctypes.c_size_t]
+        L.cbs3d_batch_step.argtypes = [vp, _i, ctypes.POINTER(StepStats), ctypes.POINTER(_d)]
+        L.cbs3d_batch_download_fields.argtypes = [vp, _i, vp, vp, vp]
+        L.cbs3d_batch_get_info.argtypes = [vp, ctypes.POINTER(BatchInfo)]
+        L.cbs3d_batch_destroy.argtypes = [vp]
+        L.cbs3d_batch_last_error.argtypes = [vp]
+        L.cbs3d_batch_last_error.restype = cp
         L.cbs3d_selftest_wait_timeout.argtypes = [_i, ctypes.POINTER(_i)]
         L.cbs3d_selftest_wait_timeout.restype = _i
         for fn in ("cbs3d_create", "cbs3d_create_from_case", "cbs3d_read_params", "cbs3d_step",
                    "cbs3d_upload_fields", "cbs3d_download_fields", "cbs3d_get_array", "cbs3d_set_array",
-                   "cbs3d_run_stage", "cbs3d_pressure_multiply", "cbs3d_pcg_create", "cbs3d_pcg_solve"):
+                   "cbs3d_run_stage", "cbs3d_pressure_multiply", "cbs3d_pcg_create", "cbs3d_pcg_solve",
+                   "cbs3d_batch_create", "cbs3d_batch_step", "cbs3d_batch_download_fields", "cbs3d_batch_get_info"):
             getattr(L, fn).restype = _i
         _lib = L
     return _lib
@@ -191,6 +211,30 @@ def make_options(precision: int = FP64, device: int = 0, inner_tol: float = 1e-5
     return o
 
 
+def _mesh_params(case):
+    """cbs3d_mesh and cbs3d_params of a generated case, plus the arrays they
+    point into (kept alive by the caller)."""
+    m = case.mesh
+    bf = np.ascontiguousarray(m.bfaces.copy())
+    if bf.size:
+        lut = np.zeros(int(bf[:, 4].max()) + 1, dtype=np.int32)
+        for raw, bc in case.bc_map.items():
+            if raw < lut.size:
+                lut[raw] = bc
+        bf[:, 4] = lut[bf[:, 4]]
+    bf = np.ascontiguousarray(bf.astype(np.int32))
+    intma = np.ascontiguousarray(m.intma, dtype=np.int32)
+    coord = np.ascontiguousarray(m.coord, dtype=np.float64)
+    mat = np.ascontiguousarray(m.mat_elem, dtype=np.int32)
+    props = [None] * 5
+    if case.params.get("material_enabled", 0) > 0:
+        pr = np.array([case.materials[int(mid)][2:] for mid in m.mat_elem], dtype=np.float64)
+        props = [np.ascontiguousarray(pr[:, i]) for i in range(5)]
+    mesh = Mesh(m.nelem, m.npoin, m.nboun, _ptr(intma), _ptr(coord), _ptr(bf), _ptr(mat),
+                *[_ptr(x) for x in props])
+    return mesh, make_params(case.params), (intma, coord, bf, mat, props)
+
+
 class Context:
     """One case resident on the GPU."""
 
@@ -205,27 +249,7 @@ class Context:
         if case_name is not None:
             rc = L.cbs3d_create_from_case(case_name.encode(), ctypes.byref(opt), ctypes.byref(self.h), err, 1024)
         else:
-            m = case.mesh
-            bf = np.ascontiguousarray(m.bfaces.copy())
-            if bf.size:
-                lut = np.zeros(int(bf[:, 4].max()) + 1, dtype=np.int32)
-                for raw, bc in case.bc_map.items():
-                    if raw < lut.size:
-                        lut[raw] = bc
-                bf[:, 4] = lut[bf[:, 4]]
-            intma = np.ascontiguousarray(m.intma, dtype=np.int32)
-            coord = np.ascontiguousarray(m.coord, dtype=np.float64)
-            mat = np.ascontiguousarray(m.mat_elem, dtype=np.int32)
-            props = [None] * 5
-            if case.params.get("material_enabled", 0) > 0:
-                pr = np.array([case.materials[int(mid)][2:] for mid in m.mat_elem], dtype=np.float64)
-                props = [np.ascontiguousarray(pr[:, i]) for i in range(5)]
-            self._keep = (intma, coord, bf, mat, props)
-            mesh = Mesh(m.nelem, m.npoin, m.nboun, _ptr(intma), _ptr(coord), _ptr(bf.astype(np.int32)),
-                        _ptr(mat), *[_ptr(x) for x in props])
-            self._keep = self._keep + (bf.astype(np.int32),)
-            mesh.bface = _ptr(self._keep[-1])
-            par = make_params(case.params)
+            mesh, par, self._keep = _mesh_params(case)
             rc = L.cbs3d_create(ctypes.byref(mesh), ctypes.byref(par), ctypes.byref(opt), ctypes.byref(self.h),
                                 err, 1024)
         if rc != 0:
@@ -373,3 +397,68 @@ class Solver:
     def state(self) -> dict:
         u, p, t = self.ctx.fields()
         return {"unkno": u.reshape(-1, 3), "pres": p, "temperature": t}
+
+
+class Batch:
+    """Many independent cases advanced together (cbs3d_batch_*): one CUDA
+    graph per step, the pressure systems solved by one cooperative launch
+    per wave of instances."""
+
+    def __init__(self, cases, precision: int = FP64, device: int = 0, autotune: bool = True,
+                 rows_per_thread: int = 4, spread: bool = True, use_graph: bool = True, inner_tol: float = 1e-5):
+        L = lib()
+        self.h = ctypes.c_void_p()
+        self.n = len(cases)
+        opt = BatchOptions()
+        L.cbs3d_default_batch_options(ctypes.byref(opt))
+        opt.base = make_options(precision, device, inner_tol, use_graph)
+        opt.autotune = 1 if autotune else 0
+        opt.rows_per_thread = rows_per_thread
+        opt.spread = 1 if spread else 0
+        meshes = (Mesh * self.n)()
+        pars = (Params * self.n)()
+        self._keep = []
+        self.npoin = []
+        for i, c in enumerate(cases):
+            m, p, keep = _mesh_params(c)
+            meshes[i] = m
+            pars[i] = p
+            self._keep.append(keep)
+            self.npoin.append(c.mesh.npoin)
+        err = ctypes.create_string_buffer(1024)
+        rc = L.cbs3d_batch_create(self.n, meshes, pars, ctypes.byref(opt), ctypes.byref(self.h), err, 1024)
+        if rc != 0:
+            self.h = None
+            raise CBSError(rc, err.value.decode())
+
+    def _check(self, rc: int):
+        if rc != 0:
+            raise CBSError(rc, lib().cbs3d_batch_last_error(self.h).decode())
+
+    def step(self, n: int = 1):
+        """n steps of every instance; returns (per-instance StepStats, device seconds)."""
+        st = (StepStats * self.n)()
+        sec = ctypes.c_double()
+        self._check(lib().cbs3d_batch_step(self.h, n, st, ctypes.byref(sec)))
+        return list(st), sec.value
+
+    def fields(self, i: int):
+        N = self.npoin[i]
+        u, p, t = np.empty(3 * N), np.empty(N), np.empty(N)
+        self._check(lib().cbs3d_batch_download_fields(self.h, i, _ptr(u), _ptr(p), _ptr(t)))
+        return u, p, t
+
+    def info(self) -> dict:
+        inf = BatchInfo()
+        self._check(lib().cbs3d_batch_get_info(self.h, ctypes.byref(inf)))
+        d = {n: getattr(inf, n) for n, _ in BatchInfo._fields_ if not n.startswith("cand_")}
+        d["candidates_timed"] = [(inf.cand_rows[k], inf.cand_spread[k], inf.cand_ms[k]) for k in range(inf.candidates)]
+        return d
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().cbs3d_batch_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        self.close()

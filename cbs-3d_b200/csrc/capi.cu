@@ -137,6 +137,7 @@ struct cbs3d_ctx {
     int pcg_ev_used = 0;
     long long launches = 0;            // kernels enqueued (counted at enqueue time)
     int step_kernels = 0;              // kernels per enqueued step
+    CgOut* batch_out = nullptr;        // member of a batch: its pressure-solve result (no own PCG engine)
 
     ~cbs3d_ctx()
     {
@@ -161,16 +162,21 @@ struct cbs3d_ctx {
                (m.p.ilots != 1 && m.p.ilots != 2);
     }
 
-    void setup();
+    void setup(bool own_pcg = true);
     void check_status();
     void reset_status() { CUDA_OK(cudaMemsetAsync(S.status, 0, sizeof(DevStatus), st)); }
     void stage_time_step(int it);
     void stage_solve();
+    // Solver::advanceOneStep in two halves around the pressure solve
+    void enqueue_pre(int it);
+    void enqueue_post(int it);
     void enqueue_step(int it);
+    // kernels of one step outside the pressure solve
+    int kernels_outside_solve(int it) const;
     void ensure_log(int n);
 };
 
-void cbs3d_ctx::setup()
+void cbs3d_ctx::setup(bool own_pcg)
 {
     CUDA_OK(cudaSetDevice(opt.device));
     CUDA_OK(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
@@ -273,6 +279,7 @@ void cbs3d_ctx::setup()
     CUDA_OK(cudaGetLastError());
     CUDA_OK(cudaStreamSynchronize(st));
     check_status();
+    if (!own_pcg) return;
     pcg.inner_tol = opt.inner_tol > 0.0 ? opt.inner_tol : 1.0e-5;
     pcg.init(m, S.nflag, S.pfix, S.status, opt.device, opt.pcg_blocks, opt.precision == CBS3D_MIXED, opt.pcg_kernel);
 }
@@ -313,7 +320,7 @@ void cbs3d_ctx::stage_solve()
               m.p.relToler, m.p.absToler, st, false, e0, e1);
 }
 
-void cbs3d_ctx::enqueue_step(int it)
+void cbs3d_ctx::enqueue_pre(int it)
 {
     k_begin_step<<<nb(m.N), T, 0, st>>>(S);
     stage_time_step(it);
@@ -326,7 +333,11 @@ void cbs3d_ctx::enqueue_step(int it)
     }
     k_step2_elem<<<nb(m.E), T, 0, st>>>(S);
     k_step2_node<<<nb(m.N), T, 0, st>>>(S);
-    stage_solve();
+}
+
+void cbs3d_ctx::enqueue_post(int it)
+{
+    (void)it;
     k_step3_elem<<<nb(m.E), T, 0, st>>>(S);
     k_step3_node<<<nb(m.N), T, 0, st>>>(S);
     if (m.temp_calc > 0) {
@@ -335,11 +346,23 @@ void cbs3d_ctx::enqueue_step(int it)
     }
     k_conv_partial<<<static_cast<unsigned>(conv_blocks), T, 0, st>>>(S);
     k_conv_finish<<<1, 15 * 32, 0, st>>>(S, conv_blocks);
-    k_step_log<<<1, 32, 0, st>>>(S, pcg.d_out, d_log, d_counter, log_cap);
-    // begin, timestep, dt_finish, lhs, step1 x2, step2 x2, assemble, step3 x2, conv x2, log (14)
-    // plus the pressure solve's launches
-    step_kernels = 14 + pcg.launches_per_solve() + (!fixed_dt(it) && force_global() ? 1 : 0) +
-                   (m.p.step2_check > 0 ? 2 : 0) + (m.temp_calc > 0 ? 2 : 0);
+    k_step_log<<<1, 32, 0, st>>>(S, batch_out ? batch_out : pcg.d_out, d_log, d_counter, log_cap);
+}
+
+int cbs3d_ctx::kernels_outside_solve(int it) const
+{
+    // begin, timestep, dt_finish, lhs, step1 x2, step2 x2, step3 x2, conv x2, log (13)
+    return 13 + (!fixed_dt(it) && force_global() ? 1 : 0) + (m.p.step2_check > 0 ? 2 : 0) +
+           (m.temp_calc > 0 ? 2 : 0);
+}
+
+void cbs3d_ctx::enqueue_step(int it)
+{
+    enqueue_pre(it);
+    stage_solve();
+    enqueue_post(it);
+    // plus the operator assembly and the pressure solve's launches
+    step_kernels = kernels_outside_solve(it) + 1 + pcg.launches_per_solve();
 }
 
 void cbs3d_ctx::ensure_log(int n)
@@ -355,8 +378,8 @@ void cbs3d_ctx::ensure_log(int n)
 // ---------------------------------------------------------------- helpers
 namespace {
 
-template <typename F>
-cbs3d_status guarded(cbs3d_ctx* c, F&& f)
+template <typename C, typename F>
+cbs3d_status guarded(C* c, F&& f)
 {
     if (!c) return CBS3D_INVALID_INPUT;
     try {
@@ -492,6 +515,50 @@ void cbs3d_destroy(cbs3d_ctx* ctx) { delete ctx; }
 
 const char* cbs3d_last_error(const cbs3d_ctx* ctx) { return ctx ? ctx->err.c_str() : "null context"; }
 
+// After a call's steps have finished on the device: the status word, the
+// per-step log (PCG iterations into the running total), and the stats.
+static DevStatus collect_call(cbs3d_ctx* c, int done, int start, long long launches0, bool steady, float ms,
+                              cbs3d_step_stats* stats)
+{
+    DevStatus s{};
+    CUDA_OK(cudaMemcpy(&s, c->S.status, sizeof s, cudaMemcpyDeviceToHost));
+    std::vector<double> log(static_cast<size_t>(done) * LOG_FIELDS);
+    if (done) CUDA_OK(cudaMemcpy(log.data(), c->d_log, log.size() * sizeof(double), cudaMemcpyDeviceToHost));
+    for (int k = 0; k < done; ++k) c->cg_total += static_cast<long long>(log[static_cast<size_t>(k) * LOG_FIELDS + 1]);
+    if (!stats) return s;
+    stats->steps_done = done;
+    stats->iitime = c->iitime;
+    stats->gpu_seconds = ms * 1.0e-3;
+    stats->steady_reached = steady ? 1 : 0;
+    stats->cg_iterations_total = c->cg_total;
+    stats->kernel_launches = c->launches - launches0;
+    if (!c->batch_out) {
+        stats->pcg_bytes_per_iter = static_cast<double>(c->pcg.bytes_per_iter());
+        stats->pcg_kernel = c->pcg.variant == 4 && c->pcg.mixed_ok ? 5 : c->pcg.variant;
+    }
+    for (int k = 0; k + 1 < c->pcg_ev_used; k += 2) {
+        float pm = 0.0f;
+        CUDA_OK(cudaEventElapsedTime(&pm, c->pcg_ev[static_cast<size_t>(k)], c->pcg_ev[static_cast<size_t>(k) + 1]));
+        stats->pcg_seconds += pm * 1.0e-3;
+        ++stats->pcg_launches;
+    }
+    if (done) {
+        const double* r = &log[static_cast<size_t>(done - 1) * LOG_FIELDS];
+        stats->dtreal = r[0];
+        stats->cg.iterations = static_cast<int>(r[1]);
+        stats->cg.initial_l2 = r[2];
+        stats->cg.final_l2 = r[3];
+        stats->cg.final_relative_l2 = r[4];
+        stats->cg.final_max_abs = r[5];
+        stats->cg.converged = static_cast<int>(r[6]);
+        stats->cg.outer_sweeps = static_cast<int>(r[23]);
+        for (int q = 0; q < 15; ++q) stats->hb[q] = r[7 + q];
+        stats->rtime = r[22];
+    }
+    if (s.code != 0) stats->failed_step = start + (s.step > 0 ? s.step : done);
+    return s;
+}
+
 cbs3d_status cbs3d_step(cbs3d_ctx* c, int nsteps, int stop_on_steady, cbs3d_step_stats* stats)
 {
     return guarded(c, [&] {
@@ -558,43 +625,9 @@ cbs3d_status cbs3d_step(cbs3d_ctx* c, int nsteps, int stop_on_steady, cbs3d_step
         }
         CUDA_OK(cudaEventRecord(c->ev1, c->st));
         CUDA_OK(cudaStreamSynchronize(c->st));
-        DevStatus s{};
-        CUDA_OK(cudaMemcpy(&s, c->S.status, sizeof s, cudaMemcpyDeviceToHost));
-        std::vector<double> log(static_cast<size_t>(done) * LOG_FIELDS);
-        if (done) CUDA_OK(cudaMemcpy(log.data(), c->d_log, log.size() * sizeof(double), cudaMemcpyDeviceToHost));
-        for (int k = 0; k < done; ++k) c->cg_total += static_cast<long long>(log[static_cast<size_t>(k) * LOG_FIELDS + 1]);
-        if (stats) {
-            float ms = 0.0f;
-            cudaEventElapsedTime(&ms, c->ev0, c->ev1);
-            stats->steps_done = done;
-            stats->iitime = c->iitime;
-            stats->gpu_seconds = ms * 1.0e-3;
-            stats->steady_reached = steady ? 1 : 0;
-            stats->cg_iterations_total = c->cg_total;
-            stats->kernel_launches = c->launches - launches0;
-            stats->pcg_bytes_per_iter = static_cast<double>(c->pcg.bytes_per_iter());
-            stats->pcg_kernel = c->pcg.variant == 4 && c->pcg.mixed_ok ? 5 : c->pcg.variant;
-            for (int k = 0; k + 1 < c->pcg_ev_used; k += 2) {
-                float pm = 0.0f;
-                CUDA_OK(cudaEventElapsedTime(&pm, c->pcg_ev[static_cast<size_t>(k)], c->pcg_ev[static_cast<size_t>(k) + 1]));
-                stats->pcg_seconds += pm * 1.0e-3;
-                ++stats->pcg_launches;
-            }
-            if (done) {
-                const double* r = &log[static_cast<size_t>(done - 1) * LOG_FIELDS];
-                stats->dtreal = r[0];
-                stats->cg.iterations = static_cast<int>(r[1]);
-                stats->cg.initial_l2 = r[2];
-                stats->cg.final_l2 = r[3];
-                stats->cg.final_relative_l2 = r[4];
-                stats->cg.final_max_abs = r[5];
-                stats->cg.converged = static_cast<int>(r[6]);
-                stats->cg.outer_sweeps = static_cast<int>(r[23]);
-                for (int q = 0; q < 15; ++q) stats->hb[q] = r[7 + q];
-                stats->rtime = r[22];
-            }
-            if (s.code != 0) stats->failed_step = start + (s.step > 0 ? s.step : done);
-        }
+        float ms = 0.0f;
+        cudaEventElapsedTime(&ms, c->ev0, c->ev1);
+        const DevStatus s = collect_call(c, done, start, launches0, steady, ms, stats);
         if (s.code != 0) {
             const int fstep = start + (s.step > 0 ? s.step : done);
             throw Error(static_cast<cbs3d_status>(s.code), reason_text(s) + " (step " + std::to_string(fstep) + ")");
@@ -942,5 +975,326 @@ cbs3d_status cbs3d_selftest_wait_timeout(int device, int* observed_status)
 }
 
 const char* cbs3d_pcg_last_error(const cbs3d_pcg* p) { return p ? p->err.c_str() : "null solver"; }
+
+}  // extern "C"
+
+// ================================================================ batch
+struct cbs3d_batch {
+    std::vector<std::unique_ptr<cbs3d_ctx>> inst;
+    cbs3d_batch_options opt{};
+    PcgBatch pcg;
+    cudaStream_t st = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr, fork_pre = nullptr, fork_post = nullptr;
+    std::vector<cudaEvent_t> done_pre, done_post;
+    cudaGraphExec_t gexec = nullptr;
+    bool graph_failed = false;
+    bool tuned = false;
+    int iitime = 0;
+    long long launches = 0;
+    cbs3d_batch_info info{};
+    std::string err;
+
+    ~cbs3d_batch()
+    {
+        if (gexec) cudaGraphExecDestroy(gexec);
+        pcg.release();
+        cudaEvent_t evs[] = {ev0, ev1, fork_pre, fork_post};
+        for (cudaEvent_t e : evs) if (e) cudaEventDestroy(e);
+        for (cudaEvent_t e : done_pre) cudaEventDestroy(e);
+        for (cudaEvent_t e : done_post) cudaEventDestroy(e);
+        inst.clear();
+        if (st) cudaStreamDestroy(st);
+    }
+
+    int kernels_per_step(int it) const
+    {
+        int n = pcg.nwaves();
+        for (const auto& c : inst) n += c->kernels_outside_solve(it) + pcg.launches_per_instance();
+        return n;
+    }
+
+    void enqueue_pre_all(int it)
+    {
+        CUDA_OK(cudaEventRecord(fork_pre, st));
+        for (size_t k = 0; k < inst.size(); ++k) {
+            cbs3d_ctx& c = *inst[k];
+            CUDA_OK(cudaStreamWaitEvent(c.st, fork_pre, 0));
+            c.enqueue_pre(it);
+        }
+    }
+    void enqueue_prepare_all()
+    {
+        for (size_t k = 0; k < inst.size(); ++k) {
+            cbs3d_ctx& c = *inst[k];
+            pcg.prepare(static_cast<int>(k), c.S, c.st);
+            CUDA_OK(cudaEventRecord(done_pre[k], c.st));
+            CUDA_OK(cudaStreamWaitEvent(st, done_pre[k], 0));
+        }
+    }
+    void enqueue_post_all(int it)
+    {
+        CUDA_OK(cudaEventRecord(fork_post, st));
+        for (size_t k = 0; k < inst.size(); ++k) {
+            cbs3d_ctx& c = *inst[k];
+            CUDA_OK(cudaStreamWaitEvent(c.st, fork_post, 0));
+            pcg.finish(static_cast<int>(k), c.S.pres, c.st);
+            c.enqueue_post(it);
+            CUDA_OK(cudaEventRecord(done_post[k], c.st));
+            CUDA_OK(cudaStreamWaitEvent(st, done_post[k], 0));
+        }
+    }
+    void enqueue_step(int it)
+    {
+        enqueue_pre_all(it);
+        enqueue_prepare_all();
+        pcg.solve(st);
+        enqueue_post_all(it);
+    }
+
+    // First step with the autotuner: the stages before the solve run once;
+    // every feasible tiling then solves the same systems (inputs re-staged
+    // each time, the node-order pressure untouched) and is timed; the fastest
+    // is kept and solves the step for real.
+    void autotune_step(int it)
+    {
+        enqueue_pre_all(it);
+        const PcgBatchPlan start = pcg.current;
+        double best = 1e300;
+        PcgBatchPlan best_plan = start;
+        int nc = 0;
+        const int rows[3] = {2, 4, 8};
+        for (int spread = 1; spread >= 0; --spread) {
+            for (int r : rows) {
+                if (nc >= 8) break;
+                PcgBatchPlan p;
+                p.rmax = r;
+                p.spread = spread;
+                info.cand_rows[nc] = r;
+                info.cand_spread[nc] = spread;
+                info.cand_ms[nc] = -1.0;
+                std::string why;
+                if (pcg.plan(p, &why)) {
+                    float ms = 1e30f;
+                    for (int rep = 0; rep < 2; ++rep) {
+                        enqueue_prepare_all();
+                        CUDA_OK(cudaEventRecord(ev0, st));
+                        pcg.solve(st);
+                        CUDA_OK(cudaEventRecord(ev1, st));
+                        CUDA_OK(cudaStreamSynchronize(st));
+                        float m = 0.0f;
+                        CUDA_OK(cudaEventElapsedTime(&m, ev0, ev1));
+                        ms = std::min(ms, m);
+                    }
+                    info.cand_ms[nc] = ms;
+                    if (ms < best) { best = ms; best_plan = p; }
+                }
+                ++nc;
+            }
+        }
+        info.candidates = nc;
+        std::string why;
+        if (!pcg.plan(best_plan, &why)) throw Error(CBS3D_INTERNAL, "batch autotuner: " + why);
+        tuned = true;
+        enqueue_prepare_all();
+        pcg.solve(st);
+        enqueue_post_all(it);
+    }
+};
+
+namespace {
+
+void batch_fill_info(cbs3d_batch* b)
+{
+    b->info.instances = static_cast<int>(b->inst.size());
+    b->info.waves = b->pcg.nwaves();
+    b->info.rows_per_thread = b->pcg.current.rmax;
+    b->info.spread = b->pcg.current.spread;
+    b->info.mixed_waves = b->pcg.mixed_any ? 1 : 0;
+    b->info.tuned = b->tuned ? 1 : 0;
+}
+
+}  // namespace
+
+extern "C" {
+
+void cbs3d_default_batch_options(cbs3d_batch_options* o)
+{
+    if (!o) return;
+    std::memset(o, 0, sizeof *o);
+    cbs3d_default_options(&o->base);
+    o->autotune = 1;
+    o->rows_per_thread = 4;
+    o->spread = 1;
+}
+
+cbs3d_status cbs3d_batch_create(int n, const cbs3d_mesh* meshes, const cbs3d_params* params,
+                                const cbs3d_batch_options* opt, cbs3d_batch** out, char* err, size_t errlen)
+{
+    if (n < 1 || !meshes || !params || !out) return CBS3D_INVALID_INPUT;
+    *out = nullptr;
+    auto b = std::make_unique<cbs3d_batch>();
+    try {
+        if (opt) b->opt = *opt; else cbs3d_default_batch_options(&b->opt);
+        const int rpt = b->opt.rows_per_thread;
+        if (rpt != 0 && rpt != 1 && rpt != 2 && rpt != 4 && rpt != 8)
+            throw Error(CBS3D_INVALID_INPUT, "cbs3d_batch_create - rows_per_thread must be 1, 2, 4 or 8");
+        CUDA_OK(cudaSetDevice(b->opt.base.device));
+        CUDA_OK(cudaStreamCreateWithFlags(&b->st, cudaStreamNonBlocking));
+        CUDA_OK(cudaEventCreate(&b->ev0));
+        CUDA_OK(cudaEventCreate(&b->ev1));
+        CUDA_OK(cudaEventCreateWithFlags(&b->fork_pre, cudaEventDisableTiming));
+        CUDA_OK(cudaEventCreateWithFlags(&b->fork_post, cudaEventDisableTiming));
+        std::vector<PcgBatchMember> mem;
+        for (int i = 0; i < n; ++i) {
+            auto c = std::make_unique<cbs3d_ctx>();
+            try {
+                model_from_arrays(meshes[i], params[i], c->m);
+                c->opt = b->opt.base;
+                c->opt.time_pcg = 0;
+                c->setup(false);
+            } catch (const Error& e) {
+                throw Error(e.code, "instance " + std::to_string(i) + ": " + e.what());
+            }
+            mem.push_back(PcgBatchMember{&c->m, c->S.nflag, c->S.pfix, c->S.status});
+            b->inst.push_back(std::move(c));
+            cudaEvent_t e1, e2;
+            CUDA_OK(cudaEventCreateWithFlags(&e1, cudaEventDisableTiming));
+            CUDA_OK(cudaEventCreateWithFlags(&e2, cudaEventDisableTiming));
+            b->done_pre.push_back(e1);
+            b->done_post.push_back(e2);
+        }
+        const double itol = b->opt.base.inner_tol > 0.0 ? b->opt.base.inner_tol : 1.0e-5;
+        b->pcg.init(mem, b->opt.base.device, b->opt.base.precision == CBS3D_MIXED, itol);
+        for (int i = 0; i < n; ++i) b->inst[static_cast<size_t>(i)]->batch_out = b->pcg.out(i);
+        PcgBatchPlan p;
+        p.rmax = b->opt.rows_per_thread > 0 ? b->opt.rows_per_thread : 4;
+        p.spread = b->opt.spread ? 1 : 0;
+        std::string why;
+        if (!b->pcg.plan(p, &why)) {
+            p.rmax = 8;   // the widest tiling holds the largest instances
+            if (!b->pcg.plan(p, &why)) throw Error(CBS3D_INVALID_INPUT, "cbs3d_batch_create - " + why);
+        }
+        batch_fill_info(b.get());
+        *out = b.release();
+        return CBS3D_OK;
+    } catch (const Error& e) {
+        fill_err(err, errlen, e.what());
+        return e.code;
+    } catch (const std::exception& e) {
+        fill_err(err, errlen, e.what());
+        return CBS3D_INTERNAL;
+    }
+}
+
+cbs3d_status cbs3d_batch_step(cbs3d_batch* b, int nsteps, cbs3d_step_stats* stats, double* gpu_seconds)
+{
+    return guarded(b, [&] {
+        if (nsteps < 0) throw Error(CBS3D_INVALID_INPUT, "cbs3d_batch_step - nsteps must be >= 0");
+        const size_t K = b->inst.size();
+        if (stats) std::memset(stats, 0, K * sizeof *stats);
+        CUDA_OK(cudaSetDevice(b->opt.base.device));
+        std::vector<int> start(K);
+        std::vector<long long> launches0(K);
+        for (size_t k = 0; k < K; ++k) {
+            cbs3d_ctx& c = *b->inst[k];
+            const bool realloc = !c.d_log || nsteps > c.log_cap;
+            c.ensure_log(nsteps > 0 ? nsteps : 1);
+            if (realloc && b->gexec) { cudaGraphExecDestroy(b->gexec); b->gexec = nullptr; }
+            c.reset_status();
+            CUDA_OK(cudaMemsetAsync(c.d_counter, 0, sizeof(int), c.st));
+            CUDA_OK(cudaStreamSynchronize(c.st));
+            start[k] = c.iitime;
+            launches0[k] = c.launches;
+            c.pcg_ev_used = 0;
+        }
+        CUDA_OK(cudaEventRecord(b->ev0, b->st));
+        int done = 0;
+        for (int s = 0; s < nsteps; ++s) {
+            const int it = b->iitime + 1;
+            bool graphable = b->opt.base.use_graph && !b->graph_failed;
+            for (const auto& c : b->inst)
+                if (c->m.p.dtfix_end > 0 && it <= c->m.p.dtfix_end) graphable = false;
+            if (b->opt.autotune && !b->tuned) {
+                // The autotuner times candidates with the same events, so the
+                // call's device time starts after the tuned step.
+                b->autotune_step(it);
+                if (b->gexec) { cudaGraphExecDestroy(b->gexec); b->gexec = nullptr; }
+                CUDA_OK(cudaStreamSynchronize(b->st));
+                CUDA_OK(cudaEventRecord(b->ev0, b->st));
+            } else {
+                if (graphable && !b->gexec) {
+                    cudaGraph_t g = nullptr;
+                    bool ok = cudaStreamBeginCapture(b->st, cudaStreamCaptureModeThreadLocal) == cudaSuccess;
+                    if (ok) {
+                        try {
+                            b->enqueue_step(it);
+                        } catch (const Error&) {
+                            ok = false;
+                        }
+                        cudaGraph_t gg = nullptr;
+                        const bool ended = cudaStreamEndCapture(b->st, &gg) == cudaSuccess && gg;
+                        g = gg;
+                        ok = ok && ended;
+                    }
+                    if (ok) ok = cudaGraphInstantiate(&b->gexec, g, 0) == cudaSuccess;
+                    if (g) cudaGraphDestroy(g);
+                    if (!ok) {
+                        cudaGetLastError();
+                        b->graph_failed = true;
+                        b->gexec = nullptr;
+                    }
+                }
+                if (graphable && b->gexec) CUDA_OK(cudaGraphLaunch(b->gexec, b->st));
+                else b->enqueue_step(it);
+            }
+            const int kn = b->kernels_per_step(it);
+            b->launches += kn;
+            for (auto& c : b->inst) {
+                c->launches += c->kernels_outside_solve(it) + b->pcg.launches_per_instance();
+                c->iitime = it;
+            }
+            CUDA_OK(cudaGetLastError());
+            b->iitime = it;
+            ++done;
+        }
+        CUDA_OK(cudaEventRecord(b->ev1, b->st));
+        CUDA_OK(cudaStreamSynchronize(b->st));
+        float ms = 0.0f;
+        cudaEventElapsedTime(&ms, b->ev0, b->ev1);
+        if (gpu_seconds) *gpu_seconds = ms * 1.0e-3;
+        batch_fill_info(b);
+        int bad = -1;
+        DevStatus first{};
+        for (size_t k = 0; k < K; ++k) {
+            const DevStatus s = collect_call(b->inst[k].get(), done, start[k], launches0[k], false, ms,
+                                             stats ? stats + k : nullptr);
+            if (s.code != 0 && bad < 0) { bad = static_cast<int>(k); first = s; }
+        }
+        if (bad >= 0) {
+            const int fstep = start[static_cast<size_t>(bad)] + (first.step > 0 ? first.step : done);
+            throw Error(static_cast<cbs3d_status>(first.code),
+                        "instance " + std::to_string(bad) + ": " + reason_text(first) + " (step " + std::to_string(fstep) + ")");
+        }
+    });
+}
+
+cbs3d_status cbs3d_batch_download_fields(cbs3d_batch* b, int instance, double* u, double* p, double* t)
+{
+    if (!b || instance < 0 || instance >= static_cast<int>(b->inst.size())) return CBS3D_INVALID_INPUT;
+    const cbs3d_status s = cbs3d_download_fields(b->inst[static_cast<size_t>(instance)].get(), u, p, t);
+    if (s != CBS3D_OK) b->err = b->inst[static_cast<size_t>(instance)]->err;
+    return s;
+}
+
+cbs3d_status cbs3d_batch_get_info(const cbs3d_batch* b, cbs3d_batch_info* info)
+{
+    if (!b || !info) return CBS3D_INVALID_INPUT;
+    *info = b->info;
+    return CBS3D_OK;
+}
+
+void cbs3d_batch_destroy(cbs3d_batch* b) { delete b; }
+
+const char* cbs3d_batch_last_error(const cbs3d_batch* b) { return b ? b->err.c_str() : "null batch"; }
 
 }  // extern "C"

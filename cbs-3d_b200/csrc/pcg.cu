@@ -23,6 +23,8 @@
 
 #include <algorithm>
 #include <cstdio>
+#include <map>
+#include <mutex>
 #include <cstring>
 #include <vector>
 
@@ -34,6 +36,24 @@ constexpr int PCG_THREADS = 256;
 constexpr int PCG_WARPS = PCG_THREADS / 32;
 
 #define CUDA_OK(x) do { cudaError_t e_ = (x); if (e_ != cudaSuccess) throw Error(CBS3D_CUDA_ERROR, std::string(#x) + ": " + cudaGetErrorString(e_)); } while (0)
+
+// The dynamic shared-memory limit is one attribute per kernel and device,
+// shared by every engine and batch in the process: it only ever grows, so a
+// smaller later request cannot invalidate an earlier engine's launches.
+cudaError_t raise_smem_limit(const void* fn, size_t smem)
+{
+    static std::mutex mu;
+    static std::map<std::pair<int, const void*>, size_t> limit;
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    std::lock_guard<std::mutex> lock(mu);
+    size_t& cur = limit[{dev, fn}];
+    if (smem <= cur) return cudaSuccess;
+    e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
+    if (e == cudaSuccess) cur = smem;
+    return e;
+}
 
 template <typename T>
 T* dalloc(size_t n)
@@ -130,6 +150,38 @@ __global__ void k_ell_multiply(PcgDev D, const double* x, double* y)
     y[i] = v;
 }
 
+// ------------------------------------------------------- solve segments
+// One cooperative launch solves one system, or -- for the batched step --
+// several independent systems at once: CTAs [cta0, cta0+ncta) of the grid
+// then own instance k's slice range [s0, s1), and every reduction, barrier,
+// status and result is per instance.  SegView is this CTA's view, with the
+// solve's scalars.
+struct SegView {
+    int G, b;      // CTAs of this CTA's solve; this CTA's index among them
+    int s0, s1;    // slice range of the solve
+    int k;         // instance, -1 for a single solve
+    int precond, conv_test, max_iter;
+    double rel_tol, abs_tol;
+};
+
+template <bool BATCH>
+__device__ __forceinline__ SegView seg_view(const PcgDev& D)
+{
+    if constexpr (!BATCH)
+        return SegView{(int)gridDim.x, (int)blockIdx.x, 0, D.nslices, -1, D.precond, D.conv_test, D.max_iter,
+                       D.rel_tol, D.abs_tol};
+    else {
+    const int k = D.cta_inst[blockIdx.x];
+    const PcgInst& I = D.inst[k];
+    return SegView{I.ncta, (int)blockIdx.x - I.cta0, I.s0, I.s1, k, I.precond, I.conv_test, I.max_iter,
+                   I.rel_tol, I.abs_tol};
+    }
+}
+__device__ __forceinline__ DevStatus* seg_status(const PcgDev& D, const SegView& g) { return g.k < 0 ? D.status : D.inst[g.k].status; }
+__device__ __forceinline__ CgOut* seg_out(const PcgDev& D, const SegView& g) { return g.k < 0 ? D.out : D.inst[g.k].out; }
+__device__ __forceinline__ unsigned* seg_bar(const PcgDev& D, const SegView& g) { return g.k < 0 ? D.bar : D.inst[g.k].bar; }
+__device__ __forceinline__ double* seg_part(const PcgDev& D, const SegView& g) { return g.k < 0 ? D.part : D.inst[g.k].part; }
+
 // ------------------------------------------------- deterministic reductions
 struct Acc4 {
     double a, b, mx, flag;
@@ -138,12 +190,13 @@ struct Acc4 {
 // Grid-wide all-reduce of (sum a, sum b, max mx, max flag) fused with the
 // grid barrier (grid_allreduce_v below).
 template <int NV, int NSUM>
-__device__ __forceinline__ bool grid_allreduce_v(double (&v)[NV], const PcgDev& D, int phase, double (&out)[NV]);
+__device__ __forceinline__ bool grid_allreduce_v(double (&v)[NV], const PcgDev& D, const SegView& g, int phase,
+                                                 double (&out)[NV]);
 
-__device__ __forceinline__ bool grid_allreduce(Acc4 v, const PcgDev& D, int phase, Acc4& out)
+__device__ __forceinline__ bool grid_allreduce(Acc4 v, const PcgDev& D, const SegView& g, int phase, Acc4& out)
 {
     double a[4] = {v.a, v.b, v.mx, v.flag}, o[4];
-    const bool ok = grid_allreduce_v<4, 2>(a, D, phase, o);
+    const bool ok = grid_allreduce_v<4, 2>(a, D, g, phase, o);
     out = Acc4{o[0], o[1], o[2], o[3]};
     return ok;
 }
@@ -155,26 +208,28 @@ __device__ __forceinline__ bool cg_converged(int test, double rel, double mx, do
     return mx <= atol || rel <= rtol;
 }
 
-__device__ __forceinline__ void cg_finish(const PcgDev& D, int it, int conv, double init, double fin,
-                                          double rel, double mx)
+__device__ __forceinline__ void cg_finish(const PcgDev& D, const SegView& g, int it, int conv, double init,
+                                          double fin, double rel, double mx)
 {
-    if (blockIdx.x == 0 && threadIdx.x == 0) {
-        D.out->iterations = it;
-        D.out->converged = conv;
-        D.out->initial_l2 = init;
-        D.out->final_l2 = fin;
-        D.out->rel = rel;
-        D.out->max_abs = mx;
+    if (g.b == 0 && threadIdx.x == 0) {
+        CgOut* o = seg_out(D, g);
+        o->iterations = it;
+        o->converged = conv;
+        o->initial_l2 = init;
+        o->final_l2 = fin;
+        o->rel = rel;
+        o->max_abs = mx;
     }
 }
 
 // ---------------------------------------------------- persistent FP64 PCG
 __global__ void __launch_bounds__(PCG_THREADS) k_pcg64(PcgDev D)
 {
-    const int G = gridDim.x, b = blockIdx.x;
+    const SegView g = seg_view<false>(D);
+    const int G = g.G, b = g.b;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int s_beg = (int)((long long)b * D.nslices / G);
-    const int s_end = (int)((long long)(b + 1) * D.nslices / G);
+    const int s_beg = g.s0 + (int)((long long)b * (g.s1 - g.s0) / G);
+    const int s_end = g.s0 + (int)((long long)(b + 1) * (g.s1 - g.s0) / G);
     int phase = 0;
     
 
@@ -193,7 +248,7 @@ __global__ void __launch_bounds__(PCG_THREADS) k_pcg64(PcgDev D)
         if (!freen) ri = 0.0;
         double zi = 0.0;
         if (freen) {
-            if (D.precond) {
+            if (g.precond) {
                 const double dg = D.pdiag[i];
                 if (!(isfinite(dg) && dg > 1.0e-30)) acc.flag = fmax(acc.flag, 1.0);
                 else zi = ri / dg;
@@ -210,21 +265,21 @@ __global__ void __launch_bounds__(PCG_THREADS) k_pcg64(PcgDev D)
         D.pA[i] = zi;
     }
     Acc4 t = Acc4{0.0, 0.0, 0.0, 0.0};
-    if (!grid_allreduce(acc, D, phase, t)) return;
+    if (!grid_allreduce(acc, D, g, phase, t)) return;
     ++phase;
     const double init = sqrt(t.a);
-    if (init <= 1.0e-300) { cg_finish(D, 0, 1, init, init, 0.0, t.mx); return; }
-    if (cg_converged(D.conv_test, 1.0, t.mx, D.rel_tol, D.abs_tol)) { cg_finish(D, 0, 1, init, init, 1.0, t.mx); return; }
-    if (t.flag >= 2.0) { if (b == 0 && threadIdx.x == 0) set_status(D.status, 4, ST_PCG, 0, R_PCG_RESID); return; }
-    if (t.flag >= 1.0) { if (b == 0 && threadIdx.x == 0) set_status(D.status, 1, ST_PCG, 0, R_PCG_DIAG); return; }
+    if (init <= 1.0e-300) { cg_finish(D, g, 0, 1, init, init, 0.0, t.mx); return; }
+    if (cg_converged(g.conv_test, 1.0, t.mx, g.rel_tol, g.abs_tol)) { cg_finish(D, g, 0, 1, init, init, 1.0, t.mx); return; }
+    if (t.flag >= 2.0) { if (b == 0 && threadIdx.x == 0) set_status(seg_status(D, g), 4, ST_PCG, 0, R_PCG_RESID); return; }
+    if (t.flag >= 1.0) { if (b == 0 && threadIdx.x == 0) set_status(seg_status(D, g), 1, ST_PCG, 0, R_PCG_DIAG); return; }
     double rz = t.b;
-    if (rz <= 1.0e-300 || !isfinite(rz)) { if (b == 0 && threadIdx.x == 0) set_status(D.status, 3, ST_PCG, 0, R_PCG_RZ0); return; }
+    if (rz <= 1.0e-300 || !isfinite(rz)) { if (b == 0 && threadIdx.x == 0) set_status(seg_status(D, g), 3, ST_PCG, 0, R_PCG_RZ0); return; }
 
     double* pc = D.pA;   // current direction
     double* pp = D.pB;   // previous direction (unused at it=1)
     double beta = 0.0, fin = init, rel = 1.0, mx = t.mx;
     int it = 0, conv = 0;
-    for (it = 1; it <= D.max_iter; ++it) {
+    for (it = 1; it <= g.max_iter; ++it) {
         // ---- q = A p (p formed here from z and the previous p), (p, q)
         Acc4 pa{0.0, 0.0, 0.0, 0.0};
         const bool upd = it > 1;
@@ -251,10 +306,10 @@ __global__ void __launch_bounds__(PCG_THREADS) k_pcg64(PcgDev D)
             if (freen) pa.a = fma(pci, qi, pa.a);
         }
         t = Acc4{0.0, 0.0, 0.0, 0.0};
-        if (!grid_allreduce(pa, D, phase, t)) return;
+        if (!grid_allreduce(pa, D, g, phase, t)) return;
         ++phase;
         const double pAp = t.a;
-        if (fabs(pAp) <= 1.0e-300 || !isfinite(pAp)) { if (b == 0 && threadIdx.x == 0) set_status(D.status, 3, ST_PCG, it, R_PCG_PAP); return; }
+        if (fabs(pAp) <= 1.0e-300 || !isfinite(pAp)) { if (b == 0 && threadIdx.x == 0) set_status(seg_status(D, g), 3, ST_PCG, it, R_PCG_PAP); return; }
         const double alpha = rz / pAp;
 
         // ---- p += alpha d, r -= alpha q, z = M^-1 r, (r,r), (r,z), max|r|
@@ -266,7 +321,7 @@ __global__ void __launch_bounds__(PCG_THREADS) k_pcg64(PcgDev D)
             D.pres[i] = fma(alpha, pc[i], D.pres[i]);
             const double ri = fma(-alpha, D.q[i], D.r[i]);
             D.r[i] = ri;
-            const double zi = D.precond ? ri / D.pdiag[i] : ri;
+            const double zi = g.precond ? ri / D.pdiag[i] : ri;
             D.z[i] = zi;
             if (!isfinite(ri)) rr.flag = 1.0;
             rr.a = fma(ri, ri, rr.a);
@@ -274,22 +329,22 @@ __global__ void __launch_bounds__(PCG_THREADS) k_pcg64(PcgDev D)
             rr.mx = fmax(rr.mx, fabs(ri));
         }
         t = Acc4{0.0, 0.0, 0.0, 0.0};
-        if (!grid_allreduce(rr, D, phase, t)) return;
+        if (!grid_allreduce(rr, D, g, phase, t)) return;
         ++phase;
         fin = sqrt(t.a);
         mx = t.mx;
         rel = fin / init;
-        if (cg_converged(D.conv_test, rel, mx, D.rel_tol, D.abs_tol)) { conv = 1; break; }
-        if (t.flag > 0.0) { if (b == 0 && threadIdx.x == 0) set_status(D.status, 4, ST_PCG, it, R_PCG_RESID); return; }
+        if (cg_converged(g.conv_test, rel, mx, g.rel_tol, g.abs_tol)) { conv = 1; break; }
+        if (t.flag > 0.0) { if (b == 0 && threadIdx.x == 0) set_status(seg_status(D, g), 4, ST_PCG, it, R_PCG_RESID); return; }
         const double rzn = t.b;
-        if (rzn <= 1.0e-300 || !isfinite(rzn)) { if (b == 0 && threadIdx.x == 0) set_status(D.status, 3, ST_PCG, it, R_PCG_RZ); return; }
+        if (rzn <= 1.0e-300 || !isfinite(rzn)) { if (b == 0 && threadIdx.x == 0) set_status(seg_status(D, g), 3, ST_PCG, it, R_PCG_RZ); return; }
         beta = rzn / rz;
         rz = rzn;
         double* tmp = pp; pp = pc; pc = tmp;
     }
-    if (it > D.max_iter) it = D.max_iter;
-    cg_finish(D, it, conv, init, fin, rel, mx);
-    if (!conv && b == 0 && threadIdx.x == 0) set_status(D.status, 2, ST_PCG, it, R_PCG_MAXIT);
+    if (it > g.max_iter) it = g.max_iter;
+    cg_finish(D, g, it, conv, init, fin, rel, mx);
+    if (!conv && b == 0 && threadIdx.x == 0) set_status(seg_status(D, g), 2, ST_PCG, it, R_PCG_MAXIT);
 }
 
 // ------------------------------------------- register-resident FP64 PCG
@@ -303,10 +358,11 @@ __global__ void __launch_bounds__(PCG_THREADS) k_pcg64(PcgDev D)
 template <int RMAX>
 __global__ void __launch_bounds__(PCG_THREADS, 2) k_pcg64r(PcgDev D)
 {
-    const int G = gridDim.x, b = blockIdx.x;
+    const SegView g = seg_view<false>(D);
+    const int G = g.G, b = g.b;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int s_beg = (int)((long long)b * D.nslices / G);
-    const int s_end = (int)((long long)(b + 1) * D.nslices / G);
+    const int s_beg = g.s0 + (int)((long long)b * (g.s1 - g.s0) / G);
+    const int s_end = g.s0 + (int)((long long)(b + 1) * (g.s1 - g.s0) / G);
     int phase = 0;
     
 
@@ -385,7 +441,7 @@ __global__ void __launch_bounds__(PCG_THREADS, 2) k_pcg64r(PcgDev D)
         if (!fr[k]) ri = 0.0;
         double zi = 0.0;
         if (fr[k]) {
-            if (D.precond) {
+            if (g.precond) {
                 if (!(isfinite(dg[k]) && dg[k] > 1.0e-30)) acc.flag = fmax(acc.flag, 1.0);
                 else zi = ri / dg[k];
             } else {
@@ -401,19 +457,19 @@ __global__ void __launch_bounds__(PCG_THREADS, 2) k_pcg64r(PcgDev D)
         D.pA[i] = 0.0;
     }
     Acc4 t = Acc4{0.0, 0.0, 0.0, 0.0};
-    if (!grid_allreduce(acc, D, phase, t)) return;
+    if (!grid_allreduce(acc, D, g, phase, t)) return;
     ++phase;
     const double init = sqrt(t.a);
-    if (init <= 1.0e-300) { cg_finish(D, 0, 1, init, init, 0.0, t.mx); return; }
-    if (cg_converged(D.conv_test, 1.0, t.mx, D.rel_tol, D.abs_tol)) { cg_finish(D, 0, 1, init, init, 1.0, t.mx); return; }
-    if (t.flag >= 2.0) { if (b == 0 && threadIdx.x == 0) set_status(D.status, 4, ST_PCG, 0, R_PCG_RESID); return; }
-    if (t.flag >= 1.0) { if (b == 0 && threadIdx.x == 0) set_status(D.status, 1, ST_PCG, 0, R_PCG_DIAG); return; }
+    if (init <= 1.0e-300) { cg_finish(D, g, 0, 1, init, init, 0.0, t.mx); return; }
+    if (cg_converged(g.conv_test, 1.0, t.mx, g.rel_tol, g.abs_tol)) { cg_finish(D, g, 0, 1, init, init, 1.0, t.mx); return; }
+    if (t.flag >= 2.0) { if (b == 0 && threadIdx.x == 0) set_status(seg_status(D, g), 4, ST_PCG, 0, R_PCG_RESID); return; }
+    if (t.flag >= 1.0) { if (b == 0 && threadIdx.x == 0) set_status(seg_status(D, g), 1, ST_PCG, 0, R_PCG_DIAG); return; }
     double rz = t.b;
-    if (rz <= 1.0e-300 || !isfinite(rz)) { if (b == 0 && threadIdx.x == 0) set_status(D.status, 3, ST_PCG, 0, R_PCG_RZ0); return; }
+    if (rz <= 1.0e-300 || !isfinite(rz)) { if (b == 0 && threadIdx.x == 0) set_status(seg_status(D, g), 3, ST_PCG, 0, R_PCG_RZ0); return; }
 
     double beta = 0.0, fin = init, rel = 1.0, mx = t.mx;
     int it = 0, conv = 0;
-    for (it = 1; it <= D.max_iter; ++it) {
+    for (it = 1; it <= g.max_iter; ++it) {
         const double* pprev = (it & 1) ? D.pA : D.pB;
         double* pnew = (it & 1) ? D.pB : D.pA;
         // ---- p = z + beta p (own rows), q = A p with neighbours' p formed on the fly
@@ -429,10 +485,10 @@ __global__ void __launch_bounds__(PCG_THREADS, 2) k_pcg64r(PcgDev D)
             if (fr[k]) pa.a = fma(p[k], q[k], pa.a);
         }
         t = Acc4{0.0, 0.0, 0.0, 0.0};
-        if (!grid_allreduce(pa, D, phase, t)) return;
+        if (!grid_allreduce(pa, D, g, phase, t)) return;
         ++phase;
         const double pAp = t.a;
-        if (fabs(pAp) <= 1.0e-300 || !isfinite(pAp)) { if (b == 0 && threadIdx.x == 0) set_status(D.status, 3, ST_PCG, it, R_PCG_PAP); return; }
+        if (fabs(pAp) <= 1.0e-300 || !isfinite(pAp)) { if (b == 0 && threadIdx.x == 0) set_status(seg_status(D, g), 3, ST_PCG, it, R_PCG_PAP); return; }
         const double alpha = rz / pAp;
 
         // ---- x += alpha p, r -= alpha q, z = M^-1 r
@@ -443,7 +499,7 @@ __global__ void __launch_bounds__(PCG_THREADS, 2) k_pcg64r(PcgDev D)
             if (i < 0 || !fr[k]) continue;
             D.pres[i] = fma(alpha, p[k], D.pres[i]);
             r[k] = fma(-alpha, q[k], r[k]);
-            const double zk = D.precond ? r[k] / dg[k] : r[k];
+            const double zk = g.precond ? r[k] / dg[k] : r[k];
             D.z[i] = zk;
             if (!isfinite(r[k])) rr.flag = 1.0;
             rr.a = fma(r[k], r[k], rr.a);
@@ -451,21 +507,21 @@ __global__ void __launch_bounds__(PCG_THREADS, 2) k_pcg64r(PcgDev D)
             rr.mx = fmax(rr.mx, fabs(r[k]));
         }
         t = Acc4{0.0, 0.0, 0.0, 0.0};
-        if (!grid_allreduce(rr, D, phase, t)) return;
+        if (!grid_allreduce(rr, D, g, phase, t)) return;
         ++phase;
         fin = sqrt(t.a);
         mx = t.mx;
         rel = fin / init;
-        if (cg_converged(D.conv_test, rel, mx, D.rel_tol, D.abs_tol)) { conv = 1; break; }
-        if (t.flag > 0.0) { if (b == 0 && threadIdx.x == 0) set_status(D.status, 4, ST_PCG, it, R_PCG_RESID); return; }
+        if (cg_converged(g.conv_test, rel, mx, g.rel_tol, g.abs_tol)) { conv = 1; break; }
+        if (t.flag > 0.0) { if (b == 0 && threadIdx.x == 0) set_status(seg_status(D, g), 4, ST_PCG, it, R_PCG_RESID); return; }
         const double rzn = t.b;
-        if (rzn <= 1.0e-300 || !isfinite(rzn)) { if (b == 0 && threadIdx.x == 0) set_status(D.status, 3, ST_PCG, it, R_PCG_RZ); return; }
+        if (rzn <= 1.0e-300 || !isfinite(rzn)) { if (b == 0 && threadIdx.x == 0) set_status(seg_status(D, g), 3, ST_PCG, it, R_PCG_RZ); return; }
         beta = rzn / rz;
         rz = rzn;
     }
-    if (it > D.max_iter) it = D.max_iter;
-    cg_finish(D, it, conv, init, fin, rel, mx);
-    if (!conv && b == 0 && threadIdx.x == 0) set_status(D.status, 2, ST_PCG, it, R_PCG_MAXIT);
+    if (it > g.max_iter) it = g.max_iter;
+    cg_finish(D, g, it, conv, init, fin, rel, mx);
+    if (!conv && b == 0 && threadIdx.x == 0) set_status(seg_status(D, g), 2, ST_PCG, it, R_PCG_MAXIT);
 }
 
 // ---------------------------------------- halo-staged FP64 PCG (default)
@@ -482,14 +538,15 @@ template <int RMAX>
 __global__ void __launch_bounds__(PCG_THREADS, 2) k_pcg64h(PcgDev D)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    const int G = gridDim.x, b = blockIdx.x;
+    const SegView g = seg_view<false>(D);
+    const int G = g.G, b = g.b;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int s_beg = (int)((long long)b * D.nslices / G);
-    const int s_end = (int)((long long)(b + 1) * D.nslices / G);
+    const int s_beg = g.s0 + (int)((long long)b * (g.s1 - g.s0) / G);
+    const int s_end = g.s0 + (int)((long long)(b + 1) * (g.s1 - g.s0) / G);
     const long long S0 = D.slice_off[s_beg];
     const int nsl = (int)(D.slice_off[s_end] - S0);
-    const int h0 = D.halo_ptr[b];
-    const int nh = D.halo_ptr[b + 1] - h0;
+    const int h0 = D.halo_ptr[blockIdx.x];
+    const int nh = D.halo_ptr[blockIdx.x + 1] - h0;
     double* vh = reinterpret_cast<double*>(smem_raw);
     int* hidx = reinterpret_cast<int*>(vh + D.halo_max);
     unsigned short* lcs = reinterpret_cast<unsigned short*>(hidx + D.halo_max);
@@ -565,7 +622,7 @@ __global__ void __launch_bounds__(PCG_THREADS, 2) k_pcg64h(PcgDev D)
         if (!fr[k]) ri = 0.0;
         double zi = 0.0;
         if (fr[k]) {
-            if (D.precond) {
+            if (g.precond) {
                 if (!(isfinite(dg[k]) && dg[k] > 1.0e-30)) acc.flag = fmax(acc.flag, 1.0);
                 else zi = ri / dg[k];
             } else {
@@ -581,19 +638,19 @@ __global__ void __launch_bounds__(PCG_THREADS, 2) k_pcg64h(PcgDev D)
         D.pA[i] = 0.0;
     }
     Acc4 t = Acc4{0.0, 0.0, 0.0, 0.0};
-    if (!grid_allreduce(acc, D, phase, t)) return;
+    if (!grid_allreduce(acc, D, g, phase, t)) return;
     ++phase;
     const double init = sqrt(t.a);
-    if (init <= 1.0e-300) { cg_finish(D, 0, 1, init, init, 0.0, t.mx); return; }
-    if (cg_converged(D.conv_test, 1.0, t.mx, D.rel_tol, D.abs_tol)) { cg_finish(D, 0, 1, init, init, 1.0, t.mx); return; }
-    if (t.flag >= 2.0) { if (b == 0 && threadIdx.x == 0) set_status(D.status, 4, ST_PCG, 0, R_PCG_RESID); return; }
-    if (t.flag >= 1.0) { if (b == 0 && threadIdx.x == 0) set_status(D.status, 1, ST_PCG, 0, R_PCG_DIAG); return; }
+    if (init <= 1.0e-300) { cg_finish(D, g, 0, 1, init, init, 0.0, t.mx); return; }
+    if (cg_converged(g.conv_test, 1.0, t.mx, g.rel_tol, g.abs_tol)) { cg_finish(D, g, 0, 1, init, init, 1.0, t.mx); return; }
+    if (t.flag >= 2.0) { if (b == 0 && threadIdx.x == 0) set_status(seg_status(D, g), 4, ST_PCG, 0, R_PCG_RESID); return; }
+    if (t.flag >= 1.0) { if (b == 0 && threadIdx.x == 0) set_status(seg_status(D, g), 1, ST_PCG, 0, R_PCG_DIAG); return; }
     double rz = t.b;
-    if (rz <= 1.0e-300 || !isfinite(rz)) { if (b == 0 && threadIdx.x == 0) set_status(D.status, 3, ST_PCG, 0, R_PCG_RZ0); return; }
+    if (rz <= 1.0e-300 || !isfinite(rz)) { if (b == 0 && threadIdx.x == 0) set_status(seg_status(D, g), 3, ST_PCG, 0, R_PCG_RZ0); return; }
 
     double beta = 0.0, fin = init, rel = 1.0, mx = t.mx;
     int it = 0, conv = 0;
-    for (it = 1; it <= D.max_iter; ++it) {
+    for (it = 1; it <= g.max_iter; ++it) {
         const double* pprev = (it & 1) ? D.pA : D.pB;
         double* pnew = (it & 1) ? D.pB : D.pA;
         Acc4 pa{0.0, 0.0, 0.0, 0.0};
@@ -609,10 +666,10 @@ __global__ void __launch_bounds__(PCG_THREADS, 2) k_pcg64h(PcgDev D)
             if (fr[k]) pa.a = fma(p[k], q[k], pa.a);
         }
         t = Acc4{0.0, 0.0, 0.0, 0.0};
-        if (!grid_allreduce(pa, D, phase, t)) return;
+        if (!grid_allreduce(pa, D, g, phase, t)) return;
         ++phase;
         const double pAp = t.a;
-        if (fabs(pAp) <= 1.0e-300 || !isfinite(pAp)) { if (b == 0 && threadIdx.x == 0) set_status(D.status, 3, ST_PCG, it, R_PCG_PAP); return; }
+        if (fabs(pAp) <= 1.0e-300 || !isfinite(pAp)) { if (b == 0 && threadIdx.x == 0) set_status(seg_status(D, g), 3, ST_PCG, it, R_PCG_PAP); return; }
         const double alpha = rz / pAp;
 
         Acc4 rr{0.0, 0.0, 0.0, 0.0};
@@ -622,7 +679,7 @@ __global__ void __launch_bounds__(PCG_THREADS, 2) k_pcg64h(PcgDev D)
             if (i < 0 || !fr[k]) continue;
             D.pres[i] = fma(alpha, p[k], D.pres[i]);
             r[k] = fma(-alpha, q[k], r[k]);
-            const double zk = D.precond ? r[k] / dg[k] : r[k];
+            const double zk = g.precond ? r[k] / dg[k] : r[k];
             D.z[i] = zk;
             if (!isfinite(r[k])) rr.flag = 1.0;
             rr.a = fma(r[k], r[k], rr.a);
@@ -630,21 +687,21 @@ __global__ void __launch_bounds__(PCG_THREADS, 2) k_pcg64h(PcgDev D)
             rr.mx = fmax(rr.mx, fabs(r[k]));
         }
         t = Acc4{0.0, 0.0, 0.0, 0.0};
-        if (!grid_allreduce(rr, D, phase, t)) return;
+        if (!grid_allreduce(rr, D, g, phase, t)) return;
         ++phase;
         fin = sqrt(t.a);
         mx = t.mx;
         rel = fin / init;
-        if (cg_converged(D.conv_test, rel, mx, D.rel_tol, D.abs_tol)) { conv = 1; break; }
-        if (t.flag > 0.0) { if (b == 0 && threadIdx.x == 0) set_status(D.status, 4, ST_PCG, it, R_PCG_RESID); return; }
+        if (cg_converged(g.conv_test, rel, mx, g.rel_tol, g.abs_tol)) { conv = 1; break; }
+        if (t.flag > 0.0) { if (b == 0 && threadIdx.x == 0) set_status(seg_status(D, g), 4, ST_PCG, it, R_PCG_RESID); return; }
         const double rzn = t.b;
-        if (rzn <= 1.0e-300 || !isfinite(rzn)) { if (b == 0 && threadIdx.x == 0) set_status(D.status, 3, ST_PCG, it, R_PCG_RZ); return; }
+        if (rzn <= 1.0e-300 || !isfinite(rzn)) { if (b == 0 && threadIdx.x == 0) set_status(seg_status(D, g), 3, ST_PCG, it, R_PCG_RZ); return; }
         beta = rzn / rz;
         rz = rzn;
     }
-    if (it > D.max_iter) it = D.max_iter;
-    cg_finish(D, it, conv, init, fin, rel, mx);
-    if (!conv && b == 0 && threadIdx.x == 0) set_status(D.status, 2, ST_PCG, it, R_PCG_MAXIT);
+    if (it > g.max_iter) it = g.max_iter;
+    cg_finish(D, g, it, conv, init, fin, rel, mx);
+    if (!conv && b == 0 && threadIdx.x == 0) set_status(seg_status(D, g), 2, ST_PCG, it, R_PCG_MAXIT);
 }
 
 // --------------------------- single-synchronisation halo PCG (default)
@@ -672,12 +729,14 @@ struct Acc6 {
 // number of all-reduces this launch has completed as `phase`.  Returns false
 // when the wait gave up (status TIMEOUT) or another CTA raised a status.
 template <int NV, int NSUM>
-__device__ __forceinline__ bool grid_allreduce_v(double (&v)[NV], const PcgDev& D, int phase, double (&out)[NV])
+__device__ __forceinline__ bool grid_allreduce_v(double (&v)[NV], const PcgDev& D, const SegView& g, int phase,
+                                                 double (&out)[NV])
 {
     static_assert(NV <= 8, "partials hold 8 doubles per CTA");
     __shared__ double sm[PCG_WARPS][NV];
     __shared__ int s_ok;
-    const int G = gridDim.x;
+    const int G = g.G;
+    DevStatus* status = seg_status(D, g);
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1)
 #pragma unroll
@@ -690,8 +749,8 @@ __device__ __forceinline__ bool grid_allreduce_v(double (&v)[NV], const PcgDev& 
 #pragma unroll
         for (int q = 0; q < NV; ++q) sm[w][q] = v[q];
     __syncthreads();
-    unsigned long long* cnt = reinterpret_cast<unsigned long long*>(D.bar);
-    double* part = D.part + (size_t)(phase & 1) * G * 8;
+    unsigned long long* cnt = reinterpret_cast<unsigned long long*>(seg_bar(D, g));
+    double* part = seg_part(D, g) + (size_t)(phase & 1) * G * 8;
     if (threadIdx.x == 0) {
         double t[NV];
 #pragma unroll
@@ -699,7 +758,7 @@ __device__ __forceinline__ bool grid_allreduce_v(double (&v)[NV], const PcgDev& 
         for (int k = 0; k < PCG_WARPS; ++k)
 #pragma unroll
             for (int q = 0; q < NV; ++q) t[q] = q < NSUM ? t[q] + sm[k][q] : fmax(t[q], sm[k][q]);
-        double* p = part + (size_t)blockIdx.x * 8;
+        double* p = part + (size_t)g.b * 8;
 #pragma unroll
         for (int q = 0; q < NV; ++q) __stcg(p + q, t[q]);
         const unsigned long long target = (unsigned long long)(phase + 1) * (unsigned long long)G;
@@ -712,15 +771,15 @@ __device__ __forceinline__ bool grid_allreduce_v(double (&v)[NV], const PcgDev& 
                 unsigned long long c;
                 asm volatile("ld.acquire.gpu.global.u64 %0, [%1];" : "=l"(c) : "l"(cnt) : "memory");
                 if (c >= target) break;
-                if (ld_relaxed_int(&D.status->code) != 0) { ok = 0; break; }
+                if (ld_relaxed_int(&status->code) != 0) { ok = 0; break; }
                 if (clock64() - t0 > (1LL << 31)) {
-                    set_status(D.status, 5 /*CBS3D_TIMEOUT*/, ST_PCG, 0, R_PCG_BARRIER);
+                    set_status(status, 5 /*CBS3D_TIMEOUT*/, ST_PCG, 0, R_PCG_BARRIER);
                     ok = 0;
                     break;
                 }
             }
         }
-        if (ok && ld_relaxed_int(&D.status->code) != 0) ok = 0;
+        if (ok && ld_relaxed_int(&status->code) != 0) ok = 0;
         s_ok = ok;
     }
     __syncthreads();
@@ -756,10 +815,10 @@ __device__ __forceinline__ bool grid_allreduce_v(double (&v)[NV], const PcgDev& 
     return ok;
 }
 
-__device__ __forceinline__ bool grid_allreduce3(Acc6 v, const PcgDev& D, int phase, Acc6& out)
+__device__ __forceinline__ bool grid_allreduce3(Acc6 v, const PcgDev& D, const SegView& g, int phase, Acc6& out)
 {
     double a[5] = {v.a, v.b, v.c, v.mx, v.flag}, o[5];
-    const bool ok = grid_allreduce_v<5, 3>(a, D, phase, o);
+    const bool ok = grid_allreduce_v<5, 3>(a, D, g, phase, o);
     out = Acc6{o[0], o[1], o[2], o[3], o[4]};
     return ok;
 }
@@ -769,26 +828,27 @@ struct Acc8 {
     double a, b, c, d, e, mx, flag;
 };
 
-__device__ __forceinline__ bool grid_allreduce5(Acc8 v, const PcgDev& D, int phase, Acc8& out)
+__device__ __forceinline__ bool grid_allreduce5(Acc8 v, const PcgDev& D, const SegView& g, int phase, Acc8& out)
 {
     double a[7] = {v.a, v.b, v.c, v.d, v.e, v.mx, v.flag}, o[7];
-    const bool ok = grid_allreduce_v<7, 5>(a, D, phase, o);
+    const bool ok = grid_allreduce_v<7, 5>(a, D, g, phase, o);
     out = Acc8{o[0], o[1], o[2], o[3], o[4], o[5], o[6]};
     return ok;
 }
 
-template <int RMAX>
+template <int RMAX, bool BATCH>
 __global__ void __launch_bounds__(PCG_THREADS, 2) k_pcg64c(PcgDev D)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    const int G = gridDim.x, b = blockIdx.x;
+    const SegView g = seg_view<BATCH>(D);
+    const int G = g.G, b = g.b;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int s_beg = (int)((long long)b * D.nslices / G);
-    const int s_end = (int)((long long)(b + 1) * D.nslices / G);
+    const int s_beg = g.s0 + (int)((long long)b * (g.s1 - g.s0) / G);
+    const int s_end = g.s0 + (int)((long long)(b + 1) * (g.s1 - g.s0) / G);
     const long long S0 = D.slice_off[s_beg];
     const int nsl = (int)(D.slice_off[s_end] - S0);
-    const int h0 = D.halo_ptr[b];
-    const int nh = D.halo_ptr[b + 1] - h0;
+    const int h0 = D.halo_ptr[blockIdx.x];
+    const int nh = D.halo_ptr[blockIdx.x + 1] - h0;
     double* vh = reinterpret_cast<double*>(smem_raw);
     double* dzh = vh + D.halo_max;
     int* hidx = reinterpret_cast<int*>(dzh + D.halo_max);
@@ -872,7 +932,7 @@ __global__ void __launch_bounds__(PCG_THREADS, 2) k_pcg64c(PcgDev D)
         double ri = active ? D.rhs1[i] - y : 0.0;
         if (!fr[k]) ri = 0.0;
         if (fr[k]) {
-            if (D.precond) {
+            if (g.precond) {
                 if (!(isfinite(pd) && pd > 1.0e-30)) acc.flag = fmax(acc.flag, 1.0);
                 dd[k] = pd;
             } else {
@@ -888,13 +948,13 @@ __global__ void __launch_bounds__(PCG_THREADS, 2) k_pcg64c(PcgDev D)
         sb[0][i] = 0.0;
     }
     Acc6 t{0.0, 0.0, 0.0, 0.0, 0.0};
-    if (!grid_allreduce3(acc, D, phase, t)) return;
+    if (!grid_allreduce3(acc, D, g, phase, t)) return;
     ++phase;
     const double init = sqrt(t.c);
-    if (init <= 1.0e-300) { cg_finish(D, 0, 1, init, init, 0.0, t.mx); return; }
-    if (cg_converged(D.conv_test, 1.0, t.mx, D.rel_tol, D.abs_tol)) { cg_finish(D, 0, 1, init, init, 1.0, t.mx); return; }
-    if (t.flag >= 2.0) { if (b == 0 && threadIdx.x == 0) set_status(D.status, 4, ST_PCG, 0, R_PCG_RESID); return; }
-    if (t.flag >= 1.0) { if (b == 0 && threadIdx.x == 0) set_status(D.status, 1, ST_PCG, 0, R_PCG_DIAG); return; }
+    if (init <= 1.0e-300) { cg_finish(D, g, 0, 1, init, init, 0.0, t.mx); return; }
+    if (cg_converged(g.conv_test, 1.0, t.mx, g.rel_tol, g.abs_tol)) { cg_finish(D, g, 0, 1, init, init, 1.0, t.mx); return; }
+    if (t.flag >= 2.0) { if (b == 0 && threadIdx.x == 0) set_status(seg_status(D, g), 4, ST_PCG, 0, R_PCG_RESID); return; }
+    if (t.flag >= 1.0) { if (b == 0 && threadIdx.x == 0) set_status(seg_status(D, g), 1, ST_PCG, 0, R_PCG_DIAG); return; }
 
     // ---- phase 0b: z0 = M^-1 r0, w0 = A z0, gamma0 = (r0,z0), delta0 = (z0,w0)
     __syncthreads();
@@ -929,15 +989,15 @@ __global__ void __launch_bounds__(PCG_THREADS, 2) k_pcg64c(PcgDev D)
         }
     }
     t = Acc6{0.0, 0.0, 0.0, 0.0, 0.0};
-    if (!grid_allreduce3(acc, D, phase, t)) return;
+    if (!grid_allreduce3(acc, D, g, phase, t)) return;
     ++phase;
     double gam = t.a;
-    if (gam <= 1.0e-300 || !isfinite(gam)) { if (b == 0 && threadIdx.x == 0) set_status(D.status, 3, ST_PCG, 0, R_PCG_RZ0); return; }
+    if (gam <= 1.0e-300 || !isfinite(gam)) { if (b == 0 && threadIdx.x == 0) set_status(seg_status(D, g), 3, ST_PCG, 0, R_PCG_RZ0); return; }
     double den = t.b;
     double beta = 0.0, fin = init, rel = 1.0, mx = 0.0, alpha = 0.0;
     int it = 0, conv = 0;
-    for (it = 1; it <= D.max_iter; ++it) {
-        if (fabs(den) <= 1.0e-300 || !isfinite(den)) { if (b == 0 && threadIdx.x == 0) set_status(D.status, 3, ST_PCG, it, R_PCG_PAP); return; }
+    for (it = 1; it <= g.max_iter; ++it) {
+        if (fabs(den) <= 1.0e-300 || !isfinite(den)) { if (b == 0 && threadIdx.x == 0) set_status(seg_status(D, g), 3, ST_PCG, it, R_PCG_PAP); return; }
         alpha = gam / den;
         const int po = (it - 1) & 1, pn = it & 1;
         // stage z_it of the halo: s = w_o + beta*s_o, r = r_o - alpha*s, z = r / dz
@@ -1001,22 +1061,22 @@ __global__ void __launch_bounds__(PCG_THREADS, 2) k_pcg64c(PcgDev D)
             }
         }
         t = Acc6{0.0, 0.0, 0.0, 0.0, 0.0};
-        if (!grid_allreduce3(a6, D, phase, t)) return;
+        if (!grid_allreduce3(a6, D, g, phase, t)) return;
         ++phase;
         fin = sqrt(t.c);
         mx = t.mx;
         rel = fin / init;
-        if (cg_converged(D.conv_test, rel, mx, D.rel_tol, D.abs_tol)) { conv = 1; break; }
-        if (t.flag > 0.0) { if (b == 0 && threadIdx.x == 0) set_status(D.status, 4, ST_PCG, it, R_PCG_RESID); return; }
+        if (cg_converged(g.conv_test, rel, mx, g.rel_tol, g.abs_tol)) { conv = 1; break; }
+        if (t.flag > 0.0) { if (b == 0 && threadIdx.x == 0) set_status(seg_status(D, g), 4, ST_PCG, it, R_PCG_RESID); return; }
         const double gn = t.a;
-        if (gn <= 1.0e-300 || !isfinite(gn)) { if (b == 0 && threadIdx.x == 0) set_status(D.status, 3, ST_PCG, it, R_PCG_RZ); return; }
+        if (gn <= 1.0e-300 || !isfinite(gn)) { if (b == 0 && threadIdx.x == 0) set_status(seg_status(D, g), 3, ST_PCG, it, R_PCG_RZ); return; }
         beta = gn / gam;
         den = t.b - beta * gn / alpha;
         gam = gn;
     }
-    if (it > D.max_iter) it = D.max_iter;
-    cg_finish(D, it, conv, init, fin, rel, mx);
-    if (!conv && b == 0 && threadIdx.x == 0) set_status(D.status, 2, ST_PCG, it, R_PCG_MAXIT);
+    if (it > g.max_iter) it = g.max_iter;
+    cg_finish(D, g, it, conv, init, fin, rel, mx);
+    if (!conv && b == 0 && threadIdx.x == 0) set_status(seg_status(D, g), 2, ST_PCG, it, R_PCG_MAXIT);
 }
 
 // ------------------------------------------- mixed-precision PCG (FP32)
@@ -1037,18 +1097,19 @@ __global__ void __launch_bounds__(PCG_THREADS, 2) k_pcg64c(PcgDev D)
 constexpr double RU_FACTOR = 0.05;
 constexpr int RU_STALL = 256;   // iterations without a correction before one is forced
 
-template <int RMAX>
+template <int RMAX, bool BATCH>
 __global__ void __launch_bounds__(PCG_THREADS, 2) k_pcg32m(PcgDev D)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    const int G = gridDim.x, b = blockIdx.x;
+    const SegView g = seg_view<BATCH>(D);
+    const int G = g.G, b = g.b;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int s_beg = (int)((long long)b * D.nslices / G);
-    const int s_end = (int)((long long)(b + 1) * D.nslices / G);
+    const int s_beg = g.s0 + (int)((long long)b * (g.s1 - g.s0) / G);
+    const int s_end = g.s0 + (int)((long long)(b + 1) * (g.s1 - g.s0) / G);
     const long long S0 = D.slice_off[s_beg];
     const int nsl = (int)(D.slice_off[s_end] - S0);
-    const int h0 = D.halo_ptr[b];
-    const int nh = D.halo_ptr[b + 1] - h0;
+    const int h0 = D.halo_ptr[blockIdx.x];
+    const int nh = D.halo_ptr[blockIdx.x + 1] - h0;
     const int HM = D.halo_max;
     double* vh64 = reinterpret_cast<double*>(smem_raw);                 // HM doubles, or:
     float* vz = reinterpret_cast<float*>(smem_raw);                     //   HM floats (z)
@@ -1216,21 +1277,21 @@ __global__ void __launch_bounds__(PCG_THREADS, 2) k_pcg32m(PcgDev D)
         fr[k] = (f & 1) && !(f & 4);
         const double pd = D.pdiag[i];
         if (fr[k]) {
-            if (D.precond && !(isfinite(pd) && pd > 1.0e-30)) acc.flag = fmax(acc.flag, 1.0);
-            dd[k] = D.precond ? (float)pd : 1.0f;
+            if (g.precond && !(isfinite(pd) && pd > 1.0e-30)) acc.flag = fmax(acc.flag, 1.0);
+            dd[k] = g.precond ? (float)pd : 1.0f;
         }
         dz[i] = dd[k];
         sb[0][i] = 0.0f;
     }
     true_residual(0, acc);
     Acc6 t{0.0, 0.0, 0.0, 0.0, 0.0};
-    if (!grid_allreduce3(acc, D, phase, t)) return;
+    if (!grid_allreduce3(acc, D, g, phase, t)) return;
     ++phase;
     const double init = sqrt(t.c);
-    if (init <= 1.0e-300) { cg_finish(D, 0, 1, init, init, 0.0, t.mx); return; }
-    if (cg_converged(D.conv_test, 1.0, t.mx, D.rel_tol, D.abs_tol)) { cg_finish(D, 0, 1, init, init, 1.0, t.mx); return; }
-    if (t.flag >= 2.0) { if (b == 0 && threadIdx.x == 0) set_status(D.status, 4, ST_PCG, 0, R_PCG_RESID); return; }
-    if (t.flag >= 1.0) { if (b == 0 && threadIdx.x == 0) set_status(D.status, 1, ST_PCG, 0, R_PCG_DIAG); return; }
+    if (init <= 1.0e-300) { cg_finish(D, g, 0, 1, init, init, 0.0, t.mx); return; }
+    if (cg_converged(g.conv_test, 1.0, t.mx, g.rel_tol, g.abs_tol)) { cg_finish(D, g, 0, 1, init, init, 1.0, t.mx); return; }
+    if (t.flag >= 2.0) { if (b == 0 && threadIdx.x == 0) set_status(seg_status(D, g), 4, ST_PCG, 0, R_PCG_RESID); return; }
+    if (t.flag >= 1.0) { if (b == 0 && threadIdx.x == 0) set_status(seg_status(D, g), 1, ST_PCG, 0, R_PCG_DIAG); return; }
     double rr_last = t.c;
 
     // ---- phase 0b: z0, w0 = A z0 (p = 0, s = 0)
@@ -1239,15 +1300,15 @@ __global__ void __launch_bounds__(PCG_THREADS, 2) k_pcg32m(PcgDev D)
     Acc8 a8{0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
     refresh_ws(0, true, a8);
     Acc8 t8{0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
-    if (!grid_allreduce5(a8, D, phase, t8)) return;
+    if (!grid_allreduce5(a8, D, g, phase, t8)) return;
     ++phase;
     double gam = t8.a;
-    if (gam <= 1.0e-300 || !isfinite(gam)) { if (b == 0 && threadIdx.x == 0) set_status(D.status, 3, ST_PCG, 0, R_PCG_RZ0); return; }
+    if (gam <= 1.0e-300 || !isfinite(gam)) { if (b == 0 && threadIdx.x == 0) set_status(seg_status(D, g), 3, ST_PCG, 0, R_PCG_RZ0); return; }
     double den = t8.b;
     double beta = 0.0, fin = init, rel = 1.0, mx = 0.0, alpha = 0.0;
     int it = 0, conv = 0, outer = 0, last_fix = 0;
-    for (it = 1; it <= D.max_iter; ++it) {
-        if (fabs(den) <= 1.0e-300 || !isfinite(den)) { if (b == 0 && threadIdx.x == 0) set_status(D.status, 3, ST_PCG, it, R_PCG_PAP); return; }
+    for (it = 1; it <= g.max_iter; ++it) {
+        if (fabs(den) <= 1.0e-300 || !isfinite(den)) { if (b == 0 && threadIdx.x == 0) set_status(seg_status(D, g), 3, ST_PCG, it, R_PCG_PAP); return; }
         alpha = gam / den;
         const float a32 = (float)alpha, b32 = (float)beta;
         const int po = (it - 1) & 1, pn = it & 1;
@@ -1309,23 +1370,23 @@ __global__ void __launch_bounds__(PCG_THREADS, 2) k_pcg32m(PcgDev D)
             }
         }
         t = Acc6{0.0, 0.0, 0.0, 0.0, 0.0};
-        if (!grid_allreduce3(a6, D, phase, t)) return;
+        if (!grid_allreduce3(a6, D, g, phase, t)) return;
         ++phase;
-        if (t.flag > 0.0) { if (b == 0 && threadIdx.x == 0) set_status(D.status, 4, ST_PCG, it, R_PCG_RESID); return; }
+        if (t.flag > 0.0) { if (b == 0 && threadIdx.x == 0) set_status(seg_status(D, g), 4, ST_PCG, it, R_PCG_RESID); return; }
         fin = sqrt(t.c);
         mx = t.mx;
         rel = fin / init;
-        const bool candidate = cg_converged(D.conv_test, rel, mx, D.rel_tol, D.abs_tol);
+        const bool candidate = cg_converged(g.conv_test, rel, mx, g.rel_tol, g.abs_tol);
         if (candidate || t.c <= RU_FACTOR * RU_FACTOR * rr_last || it - last_fix >= RU_STALL) {
             // residual replacement from the FP64 coefficients and pressure
             Acc6 u1{0.0, 0.0, 0.0, 0.0, 0.0};
             true_residual(pn, u1);
             t = Acc6{0.0, 0.0, 0.0, 0.0, 0.0};
-            if (!grid_allreduce3(u1, D, phase, t)) return;
+            if (!grid_allreduce3(u1, D, g, phase, t)) return;
             ++phase;
             ++outer;
             last_fix = it;
-            if (t.flag > 0.0) { if (b == 0 && threadIdx.x == 0) set_status(D.status, 4, ST_PCG, it, R_PCG_RESID); return; }
+            if (t.flag > 0.0) { if (b == 0 && threadIdx.x == 0) set_status(seg_status(D, g), 4, ST_PCG, it, R_PCG_RESID); return; }
             fin = sqrt(t.c);
             mx = t.mx;
             rel = fin / init;
@@ -1333,14 +1394,14 @@ __global__ void __launch_bounds__(PCG_THREADS, 2) k_pcg32m(PcgDev D)
             // the FP32 recurrences have lost the Krylov relations, restart
             const bool restart = t.c >= rr_last;
             rr_last = t.c;
-            if (cg_converged(D.conv_test, rel, mx, D.rel_tol, D.abs_tol)) { conv = 1; break; }
+            if (cg_converged(g.conv_test, rel, mx, g.rel_tol, g.abs_tol)) { conv = 1; break; }
             Acc8 u2{0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
             refresh_ws(pn, restart, u2);
             t8 = Acc8{0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
-            if (!grid_allreduce5(u2, D, phase, t8)) return;
+            if (!grid_allreduce5(u2, D, g, phase, t8)) return;
             ++phase;
             const double gn = t8.a;
-            if (gn <= 1.0e-300 || !isfinite(gn)) { if (b == 0 && threadIdx.x == 0) set_status(D.status, 3, ST_PCG, it, R_PCG_RZ); return; }
+            if (gn <= 1.0e-300 || !isfinite(gn)) { if (b == 0 && threadIdx.x == 0) set_status(seg_status(D, g), 3, ST_PCG, it, R_PCG_RZ); return; }
             // next direction z + beta p with its curvature computed, not recurred
             beta = restart ? 0.0 : gn / gam;
             den = t8.b + beta * (t8.c + t8.d) + beta * beta * t8.e;
@@ -1348,15 +1409,15 @@ __global__ void __launch_bounds__(PCG_THREADS, 2) k_pcg32m(PcgDev D)
             continue;
         }
         const double gn = t.a;
-        if (gn <= 1.0e-300 || !isfinite(gn)) { if (b == 0 && threadIdx.x == 0) set_status(D.status, 3, ST_PCG, it, R_PCG_RZ); return; }
+        if (gn <= 1.0e-300 || !isfinite(gn)) { if (b == 0 && threadIdx.x == 0) set_status(seg_status(D, g), 3, ST_PCG, it, R_PCG_RZ); return; }
         beta = gn / gam;
         den = t.b - beta * gn / alpha;
         gam = gn;
     }
-    if (it > D.max_iter) it = D.max_iter;
-    cg_finish(D, it, conv, init, fin, rel, mx);
-    if (b == 0 && threadIdx.x == 0) D.out->outer = outer;
-    if (!conv && b == 0 && threadIdx.x == 0) set_status(D.status, 2, ST_PCG, it, R_PCG_MAXIT);
+    if (it > g.max_iter) it = g.max_iter;
+    cg_finish(D, g, it, conv, init, fin, rel, mx);
+    if (b == 0 && threadIdx.x == 0) seg_out(D, g)->outer = outer;
+    if (!conv && b == 0 && threadIdx.x == 0) set_status(seg_status(D, g), 2, ST_PCG, it, R_PCG_MAXIT);
 }
 
 // Self-test of the bounded device wait: CTA 0 leaves without arriving, so the
@@ -1455,8 +1516,8 @@ void PcgEngine::init(const HostModel& m, const uint8_t* nflag, const double* pfi
     if (kernel_choice == 0 || kernel_choice == 3 || kernel_choice == 4) {
         const void* hc3[4] = {reinterpret_cast<const void*>(k_pcg64h<1>), reinterpret_cast<const void*>(k_pcg64h<2>),
                               reinterpret_cast<const void*>(k_pcg64h<4>), reinterpret_cast<const void*>(k_pcg64h<8>)};
-        const void* hc4[4] = {reinterpret_cast<const void*>(k_pcg64c<1>), reinterpret_cast<const void*>(k_pcg64c<2>),
-                              reinterpret_cast<const void*>(k_pcg64c<4>), reinterpret_cast<const void*>(k_pcg64c<8>)};
+        const void* hc4[4] = {reinterpret_cast<const void*>(k_pcg64c<1, false>), reinterpret_cast<const void*>(k_pcg64c<2, false>),
+                              reinterpret_cast<const void*>(k_pcg64c<4, false>), reinterpret_cast<const void*>(k_pcg64c<8, false>)};
         const int want = kernel_choice == 3 ? 3 : 4;
         for (int c = 0; c < 4 && variant == 1; ++c) {
             const void* fn = want == 4 ? hc4[c] : hc3[c];
@@ -1493,7 +1554,7 @@ void PcgEngine::init(const HostModel& m, const uint8_t* nflag, const double* pfi
             if (!fits) continue;
             const size_t smem = static_cast<size_t>(hmax) * (want == 4 ? 20 : 12) + static_cast<size_t>(smax) * 2 + 16;
             if (smem > 200 * 1024) continue;
-            CUDA_OK(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
+            CUDA_OK(raise_smem_limit(fn, smem));
             CUDA_OK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, PCG_THREADS, smem));
             if (per_sm * sms < g) continue;
             variant = want;
@@ -1509,12 +1570,12 @@ void PcgEngine::init(const HostModel& m, const uint8_t* nflag, const double* pfi
             dev_halo_max = hmax;
             dev_slot_max = static_cast<int>(smax);
             if (mixed && want == 4) {
-                const void* mc[4] = {reinterpret_cast<const void*>(k_pcg32m<1>), reinterpret_cast<const void*>(k_pcg32m<2>),
-                                     reinterpret_cast<const void*>(k_pcg32m<4>), reinterpret_cast<const void*>(k_pcg32m<8>)};
+                const void* mc[4] = {reinterpret_cast<const void*>(k_pcg32m<1, false>), reinterpret_cast<const void*>(k_pcg32m<2, false>),
+                                     reinterpret_cast<const void*>(k_pcg32m<4, false>), reinterpret_cast<const void*>(k_pcg32m<8, false>)};
                 const size_t ms = static_cast<size_t>(hmax) * 16 + static_cast<size_t>(smax) * 6 + 16;
                 int per = 0;
                 if (ms <= 220 * 1024 &&
-                    cudaFuncSetAttribute(mc[c], cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(ms)) == cudaSuccess &&
+                    raise_smem_limit(mc[c], ms) == cudaSuccess &&
                     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, mc[c], PCG_THREADS, ms) == cudaSuccess &&
                     per * sms >= g) {
                     mixed_ok = true;
@@ -1616,16 +1677,16 @@ cbs3d_status PcgEngine::solve(double* pres, double* rhs1, double* pdiag, int pre
         else fn = reinterpret_cast<const void*>(k_pcg64h<8>);
         smem = halo_smem;
     } else if (variant == 4 && mixed_ok) {
-        if (rmax == 1) fn = reinterpret_cast<const void*>(k_pcg32m<1>);
-        else if (rmax == 2) fn = reinterpret_cast<const void*>(k_pcg32m<2>);
-        else if (rmax == 4) fn = reinterpret_cast<const void*>(k_pcg32m<4>);
-        else fn = reinterpret_cast<const void*>(k_pcg32m<8>);
+        if (rmax == 1) fn = reinterpret_cast<const void*>(k_pcg32m<1, false>);
+        else if (rmax == 2) fn = reinterpret_cast<const void*>(k_pcg32m<2, false>);
+        else if (rmax == 4) fn = reinterpret_cast<const void*>(k_pcg32m<4, false>);
+        else fn = reinterpret_cast<const void*>(k_pcg32m<8, false>);
         smem = mixed_smem;
     } else if (variant == 4) {
-        if (rmax == 1) fn = reinterpret_cast<const void*>(k_pcg64c<1>);
-        else if (rmax == 2) fn = reinterpret_cast<const void*>(k_pcg64c<2>);
-        else if (rmax == 4) fn = reinterpret_cast<const void*>(k_pcg64c<4>);
-        else fn = reinterpret_cast<const void*>(k_pcg64c<8>);
+        if (rmax == 1) fn = reinterpret_cast<const void*>(k_pcg64c<1, false>);
+        else if (rmax == 2) fn = reinterpret_cast<const void*>(k_pcg64c<2, false>);
+        else if (rmax == 4) fn = reinterpret_cast<const void*>(k_pcg64c<4, false>);
+        else fn = reinterpret_cast<const void*>(k_pcg64c<8, false>);
         smem = halo_smem;
     }
     if (ev0) CUDA_OK(cudaEventRecord(ev0, st));
@@ -1684,6 +1745,324 @@ size_t PcgEngine::bytes_per_iter() const
     // row (16 B), pdiag (8), new p written (8), q written (8), node flag (1).
     // Phase B: q, r, pres, pdiag read (32), r, pres, z written (24).
     return static_cast<size_t>(nnz_offdiag) * 12 + static_cast<size_t>(N) * 97;
+}
+
+// ================================================================ batch
+void PcgBatch::init(const std::vector<PcgBatchMember>& members, int dev_id, bool mixed_mode, double inner_tol)
+{
+    mem = members;
+    device = dev_id;
+    mixed = mixed_mode;
+    const size_t K = mem.size();
+    CUDA_OK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
+    gmax = 2 * sms;   // two 256-thread CTAs per SM at 128 registers
+    slice0.assign(K, 0); nsl.assign(K, 0); N_k.assign(K, 0);
+    slot0.assign(K, 0); nslot.assign(K, 0);
+    nslices = 0; nslots = 0;
+    for (size_t k = 0; k < K; ++k) {
+        const PressurePattern& P = mem[k].m->pat;
+        slice0[k] = nslices; nsl[k] = P.nslices; N_k[k] = mem[k].m->N;
+        slot0[k] = nslots; nslot[k] = P.nslots;
+        nslices += P.nslices;
+        nslots += P.nslots;
+    }
+    NP = nslices * 32;
+    // concatenated pattern: global slot offsets, widths, columns as global
+    // row positions, and each position's instance-local node
+    h_slice_off.assign(static_cast<size_t>(nslices) + 1, 0);
+    std::vector<int> sw(static_cast<size_t>(nslices), 0), rn(static_cast<size_t>(NP), -1);
+    h_col.assign(static_cast<size_t>(nslots), 0);
+    for (size_t k = 0; k < K; ++k) {
+        const PressurePattern& P = mem[k].m->pat;
+        const int p0 = slice0[k] * 32;
+        std::vector<int> pos_of(static_cast<size_t>(N_k[k]), 0);
+        for (size_t p = 0; p < P.row_node.size(); ++p) {
+            rn[static_cast<size_t>(p0) + p] = P.row_node[p];
+            if (P.row_node[p] >= 0) pos_of[static_cast<size_t>(P.row_node[p])] = p0 + static_cast<int>(p);
+        }
+        for (int s = 0; s < P.nslices; ++s) {
+            h_slice_off[static_cast<size_t>(slice0[k] + s)] = slot0[k] + P.slice_off[static_cast<size_t>(s)];
+            sw[static_cast<size_t>(slice0[k] + s)] = P.slice_w[static_cast<size_t>(s)];
+        }
+        for (long long t = 0; t < P.nslots; ++t)
+            h_col[static_cast<size_t>(slot0[k] + t)] = pos_of[static_cast<size_t>(P.col[static_cast<size_t>(t)])];
+        long long* cp = dalloc<long long>(P.cptr.size());
+        int* ce = dalloc<int>(P.cent.size());
+        CUDA_OK(cudaMemcpy(cp, P.cptr.data(), P.cptr.size() * sizeof(long long), cudaMemcpyHostToDevice));
+        if (!P.cent.empty()) CUDA_OK(cudaMemcpy(ce, P.cent.data(), P.cent.size() * sizeof(int), cudaMemcpyHostToDevice));
+        d_cptr.push_back(cp);
+        d_cent.push_back(ce);
+    }
+    h_slice_off[static_cast<size_t>(nslices)] = nslots;
+    d_slice_off = dalloc<long long>(h_slice_off.size());
+    d_slice_w = dalloc<int>(sw.size());
+    d_col = dalloc<int>(h_col.size());
+    d_row_node = dalloc<int>(rn.size());
+    CUDA_OK(cudaMemcpy(d_slice_off, h_slice_off.data(), h_slice_off.size() * sizeof(long long), cudaMemcpyHostToDevice));
+    CUDA_OK(cudaMemcpy(d_slice_w, sw.data(), sw.size() * sizeof(int), cudaMemcpyHostToDevice));
+    if (!h_col.empty()) CUDA_OK(cudaMemcpy(d_col, h_col.data(), h_col.size() * sizeof(int), cudaMemcpyHostToDevice));
+    CUDA_OK(cudaMemcpy(d_row_node, rn.data(), rn.size() * sizeof(int), cudaMemcpyHostToDevice));
+    d_lcol = dalloc<unsigned short>(static_cast<size_t>(nslots));
+    d_val = dalloc<double>(static_cast<size_t>(nslots));
+    CUDA_OK(cudaMemset(d_val, 0, static_cast<size_t>(nslots ? nslots : 1) * sizeof(double)));
+    const size_t n = static_cast<size_t>(NP);
+    d_r = dalloc<double>(2 * n); d_q = dalloc<double>(2 * n);
+    d_z = dalloc<double>(n); d_pA = dalloc<double>(n); d_pB = dalloc<double>(n);
+    d_xp = dalloc<double>(n); d_bp = dalloc<double>(n); d_dp = dalloc<double>(n);
+    d_fp = dalloc<uint8_t>(n);
+    CUDA_OK(cudaMemset(d_pB, 0, n * sizeof(double)));
+    if (mixed) {
+        d_val32 = dalloc<float>(static_cast<size_t>(nslots));
+        d_f32 = dalloc<float>(8 * n);
+        CUDA_OK(cudaMemset(d_f32, 0, 8 * n * sizeof(float)));
+    }
+    d_part = dalloc<double>(K * static_cast<size_t>(gmax) * 16);
+    d_bar = dalloc<unsigned>(4 * K);
+    d_out = dalloc<CgOut>(K);
+    CUDA_OK(cudaMemset(d_bar, 0, 4 * K * sizeof(unsigned)));
+    CUDA_OK(cudaMemset(d_out, 0, K * sizeof(CgOut)));
+
+    base = PcgDev{};
+    base.N = NP; base.nslices = nslices; base.inner_tol = inner_tol;
+    base.slice_off = d_slice_off; base.slice_w = d_slice_w; base.col = d_col; base.val = d_val;
+    base.val32 = d_val32; base.row_node = d_row_node;
+    base.pres = d_xp; base.rhs1 = d_bp; base.pdiag = d_dp; base.nflag = d_fp;
+    base.r = d_r; base.z = d_z; base.pA = d_pA; base.pB = d_pB; base.q = d_q;
+    if (mixed) {
+        base.r32 = d_f32; base.w32 = d_f32 + 2 * n; base.s32 = d_f32 + 4 * n;
+        base.p32 = d_f32 + 6 * n; base.dz32 = d_f32 + 7 * n;
+    }
+    base.lcol = d_lcol;
+}
+
+void PcgBatch::free_waves()
+{
+    for (Wave& w : waves) {
+        void* ptrs[] = {w.d_cta_inst, w.d_inst, w.d_hptr, w.d_hidx};
+        for (void* p : ptrs) if (p) cudaFree(p);
+    }
+    waves.clear();
+}
+
+bool PcgBatch::plan(const PcgBatchPlan& p, std::string* why)
+{
+    if (p.rmax != 1 && p.rmax != 2 && p.rmax != 4 && p.rmax != 8) {
+        if (why) *why = "rows per thread must be 1, 2, 4 or 8";
+        return false;
+    }
+    const int K = static_cast<int>(mem.size());
+    const int cap = PCG_WARPS * p.rmax;   // slices one CTA holds in registers
+    std::vector<int> minc(static_cast<size_t>(K));
+    for (int k = 0; k < K; ++k) {
+        minc[static_cast<size_t>(k)] = std::max(1, (nsl[static_cast<size_t>(k)] + cap - 1) / cap);
+        if (minc[static_cast<size_t>(k)] > gmax) {
+            if (why) *why = "instance " + std::to_string(k) + " needs more CTAs than one launch holds at this tiling";
+            return false;
+        }
+    }
+    // first-fit decreasing by slices into waves of at most gmax CTAs
+    std::vector<int> order(static_cast<size_t>(K));
+    for (int k = 0; k < K; ++k) order[static_cast<size_t>(k)] = k;
+    std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return nsl[static_cast<size_t>(a)] > nsl[static_cast<size_t>(b)]; });
+    std::vector<std::vector<int>> packs;
+    std::vector<int> used;
+    for (int k : order) {
+        size_t w = 0;
+        while (w < packs.size() && used[w] + minc[static_cast<size_t>(k)] > gmax) ++w;
+        if (w == packs.size()) { packs.emplace_back(); used.push_back(0); }
+        packs[w].push_back(k);
+        used[w] += minc[static_cast<size_t>(k)];
+    }
+    const void* c64[4] = {reinterpret_cast<const void*>(k_pcg64c<1, true>), reinterpret_cast<const void*>(k_pcg64c<2, true>),
+                          reinterpret_cast<const void*>(k_pcg64c<4, true>), reinterpret_cast<const void*>(k_pcg64c<8, true>)};
+    const void* c32[4] = {reinterpret_cast<const void*>(k_pcg32m<1, true>), reinterpret_cast<const void*>(k_pcg32m<2, true>),
+                          reinterpret_cast<const void*>(k_pcg32m<4, true>), reinterpret_cast<const void*>(k_pcg32m<8, true>)};
+    const int ci = p.rmax == 1 ? 0 : p.rmax == 2 ? 1 : p.rmax == 4 ? 2 : 3;
+
+    struct HostWave {
+        int G = 0, hmax = 0;
+        long long smax = 0;
+        std::vector<int> cta_inst, hptr, hidx;
+        std::vector<PcgInst> inst;
+    };
+    std::vector<HostWave> hw(packs.size());
+    std::vector<unsigned short> lcol(static_cast<size_t>(nslots), 0);
+    for (size_t w = 0; w < packs.size(); ++w) {
+        HostWave& H = hw[w];
+        const std::vector<int>& mk = packs[w];
+        std::vector<int> G(mk.size());
+        int tot = 0;
+        for (size_t j = 0; j < mk.size(); ++j) { G[j] = minc[static_cast<size_t>(mk[j])]; tot += G[j]; }
+        if (p.spread) {
+            // spare CTAs, one at a time, to the instance with the most slices per CTA
+            while (tot < gmax) {
+                int best = -1;
+                double bw = 0.0;
+                for (size_t j = 0; j < mk.size(); ++j) {
+                    if (G[j] >= nsl[static_cast<size_t>(mk[j])]) continue;
+                    const double wpc = static_cast<double>(nsl[static_cast<size_t>(mk[j])]) / G[j];
+                    if (wpc > bw) { bw = wpc; best = static_cast<int>(j); }
+                }
+                if (best < 0) break;
+                ++G[static_cast<size_t>(best)];
+                ++tot;
+            }
+        }
+        H.G = tot;
+        H.hptr.push_back(0);
+        int cta = 0;
+        for (size_t j = 0; j < mk.size(); ++j) {
+            const int k = mk[j];
+            const PressurePattern& P = mem[static_cast<size_t>(k)].m->pat;
+            PcgInst I{};
+            I.cta0 = cta; I.ncta = G[j];
+            I.s0 = slice0[static_cast<size_t>(k)]; I.s1 = I.s0 + nsl[static_cast<size_t>(k)];
+            I.precond = mem[static_cast<size_t>(k)].m->p.cg_preconditioner;
+            I.conv_test = mem[static_cast<size_t>(k)].m->p.cg_conv_test;
+            I.max_iter = mem[static_cast<size_t>(k)].m->p.cg_max_iter;
+            I.rel_tol = mem[static_cast<size_t>(k)].m->p.relToler;
+            I.abs_tol = mem[static_cast<size_t>(k)].m->p.absToler;
+            I.bar = d_bar + 4 * k;
+            I.part = d_part + static_cast<size_t>(k) * static_cast<size_t>(gmax) * 16;
+            I.status = mem[static_cast<size_t>(k)].d_status;
+            I.out = d_out + k;
+            H.inst.push_back(I);
+            (void)P;
+            std::vector<int> cols;
+            for (int b = 0; b < G[j]; ++b) {
+                H.cta_inst.push_back(static_cast<int>(j));
+                const int sb = I.s0 + static_cast<int>(static_cast<long long>(b) * (I.s1 - I.s0) / G[j]);
+                const int se = I.s0 + static_cast<int>(static_cast<long long>(b + 1) * (I.s1 - I.s0) / G[j]);
+                const long long a0 = h_slice_off[static_cast<size_t>(sb)], a1 = h_slice_off[static_cast<size_t>(se)];
+                cols.assign(h_col.begin() + a0, h_col.begin() + a1);
+                std::sort(cols.begin(), cols.end());
+                cols.erase(std::unique(cols.begin(), cols.end()), cols.end());
+                if (cols.size() > 65535) {
+                    if (why) *why = "a CTA halo exceeds 65535 columns";
+                    return false;
+                }
+                for (long long t = a0; t < a1; ++t)
+                    lcol[static_cast<size_t>(t)] = static_cast<unsigned short>(
+                        std::lower_bound(cols.begin(), cols.end(), h_col[static_cast<size_t>(t)]) - cols.begin());
+                H.hidx.insert(H.hidx.end(), cols.begin(), cols.end());
+                H.hptr.push_back(static_cast<int>(H.hidx.size()));
+                H.hmax = std::max(H.hmax, static_cast<int>(cols.size()));
+                H.smax = std::max(H.smax, a1 - a0);
+            }
+            cta += G[j];
+        }
+    }
+    // kernels and shared memory of every wave, before anything is replaced
+    std::vector<Wave> nw(hw.size());
+    for (size_t w = 0; w < hw.size(); ++w) {
+        const HostWave& H = hw[w];
+        Wave& W = nw[w];
+        W.G = H.G; W.rmax = p.rmax;
+        const size_t s64 = static_cast<size_t>(H.hmax) * 20 + static_cast<size_t>(H.smax) * 2 + 16;
+        const size_t s32 = static_cast<size_t>(H.hmax) * 16 + static_cast<size_t>(H.smax) * 6 + 16;
+        auto fits = [&](const void* fn, size_t smem) {
+            if (smem > 220 * 1024) return false;
+            if (raise_smem_limit(fn, smem) != cudaSuccess) {
+                cudaGetLastError();
+                return false;
+            }
+            int per = 0;
+            if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, fn, PCG_THREADS, smem) != cudaSuccess) {
+                cudaGetLastError();
+                return false;
+            }
+            return per * sms >= H.G;
+        };
+        if (mixed && fits(c32[ci], s32)) { W.mixed = true; W.fn = c32[ci]; W.smem = s32; }
+        else if (fits(c64[ci], s64)) { W.mixed = false; W.fn = c64[ci]; W.smem = s64; }
+        else {
+            if (why) *why = "a wave does not fit co-resident at this tiling";
+            return false;
+        }
+    }
+    free_waves();
+    mixed_any = false;
+    CUDA_OK(cudaMemcpy(d_lcol, lcol.data(), lcol.size() * sizeof(unsigned short), cudaMemcpyHostToDevice));
+    for (size_t w = 0; w < hw.size(); ++w) {
+        const HostWave& H = hw[w];
+        Wave& W = nw[w];
+        W.d_cta_inst = dalloc<int>(H.cta_inst.size());
+        W.d_inst = dalloc<PcgInst>(H.inst.size());
+        W.d_hptr = dalloc<int>(H.hptr.size());
+        W.d_hidx = dalloc<int>(H.hidx.size());
+        CUDA_OK(cudaMemcpy(W.d_cta_inst, H.cta_inst.data(), H.cta_inst.size() * sizeof(int), cudaMemcpyHostToDevice));
+        CUDA_OK(cudaMemcpy(W.d_inst, H.inst.data(), H.inst.size() * sizeof(PcgInst), cudaMemcpyHostToDevice));
+        CUDA_OK(cudaMemcpy(W.d_hptr, H.hptr.data(), H.hptr.size() * sizeof(int), cudaMemcpyHostToDevice));
+        if (!H.hidx.empty()) CUDA_OK(cudaMemcpy(W.d_hidx, H.hidx.data(), H.hidx.size() * sizeof(int), cudaMemcpyHostToDevice));
+        W.dev = base;
+        W.dev.nblocks = W.G;
+        W.dev.cta_inst = W.d_cta_inst;
+        W.dev.inst = W.d_inst;
+        W.dev.halo_ptr = W.d_hptr;
+        W.dev.halo_idx = W.d_hidx;
+        W.dev.halo_max = H.hmax;
+        W.dev.slot_max = static_cast<int>(H.smax);
+        mixed_any = mixed_any || W.mixed;
+    }
+    waves = std::move(nw);
+    current = p;
+    return true;
+}
+
+void PcgBatch::release()
+{
+    free_waves();
+    for (long long* p : d_cptr) cudaFree(p);
+    for (int* p : d_cent) cudaFree(p);
+    d_cptr.clear();
+    d_cent.clear();
+    void* ptrs[] = {d_slice_off, d_slice_w, d_col, d_row_node, d_lcol, d_val, d_val32, d_r, d_z, d_pA, d_pB, d_q,
+                    d_xp, d_bp, d_dp, d_fp, d_f32, d_part, d_bar, d_out};
+    for (void* p : ptrs) if (p) cudaFree(p);
+    d_slice_off = nullptr; d_slice_w = d_col = d_row_node = nullptr; d_lcol = nullptr; d_val = nullptr;
+    d_val32 = nullptr; d_r = d_z = d_pA = d_pB = d_q = nullptr; d_xp = d_bp = d_dp = nullptr; d_fp = nullptr;
+    d_f32 = nullptr; d_part = nullptr; d_bar = nullptr; d_out = nullptr;
+}
+
+void PcgBatch::prepare(int k, const DevState& S, cudaStream_t st)
+{
+    const size_t kk = static_cast<size_t>(k);
+    const int T = 256;
+    if (nslot[kk])
+        k_ell_from_state<<<static_cast<unsigned>((nslot[kk] + T - 1) / T), T, 0, st>>>(
+            S, d_cptr[kk], d_cent[kk], d_val + slot0[kk], d_val32 ? d_val32 + slot0[kk] : nullptr, nslot[kk]);
+    PcgDev D = base;
+    D.NN = N_k[kk];
+    D.nflag = mem[kk].d_nflag;
+    D.pfix = mem[kk].d_pfix;
+    D.pres = S.pres; D.rhs1 = S.rhs1; D.pdiag = S.pdiag;
+    k_impose<<<(N_k[kk] + T - 1) / T, T, 0, st>>>(D);
+    const int p0 = slice0[kk] * 32, np = nsl[kk] * 32;
+    D.N = np;
+    D.row_node = d_row_node + p0;
+    k_perm_in<<<(np + T - 1) / T, T, 0, st>>>(D, S.pres, S.rhs1, S.pdiag, mem[kk].d_nflag, d_xp + p0, d_bp + p0,
+                                               d_dp + p0, d_fp + p0);
+}
+
+void PcgBatch::solve(cudaStream_t st)
+{
+    CUDA_OK(cudaMemsetAsync(d_bar, 0, 4 * mem.size() * sizeof(unsigned), st));
+    CUDA_OK(cudaMemsetAsync(d_out, 0, mem.size() * sizeof(CgOut), st));
+    for (Wave& W : waves) {
+        void* args[] = {&W.dev};
+        CUDA_OK(cudaLaunchCooperativeKernel(W.fn, dim3(static_cast<unsigned>(W.G)), dim3(PCG_THREADS), args, W.smem, st));
+    }
+}
+
+void PcgBatch::finish(int k, double* pres, cudaStream_t st)
+{
+    const size_t kk = static_cast<size_t>(k);
+    const int T = 256;
+    const int p0 = slice0[kk] * 32, np = nsl[kk] * 32;
+    PcgDev D = base;
+    D.N = np;
+    D.row_node = d_row_node + p0;
+    k_perm_out<<<(np + T - 1) / T, T, 0, st>>>(D, d_xp + p0, pres);
 }
 
 }  // namespace cbs3d

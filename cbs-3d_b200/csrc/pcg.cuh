@@ -7,6 +7,7 @@
 #include "host_model.h"
 
 #include <cuda_runtime.h>
+#include <string>
 #include <vector>
 
 namespace cbs3d {
@@ -17,6 +18,18 @@ struct CgOut {
     int outer;
     int pad;
     double initial_l2, final_l2, rel, max_abs;
+};
+
+// One instance of a batched solve: CTAs [cta0, cta0+ncta) of the launch own
+// slices [s0, s1); its own scalars, barrier counter, partials, status, result.
+struct PcgInst {
+    int cta0, ncta, s0, s1;
+    int precond, conv_test, max_iter, pad;
+    double rel_tol, abs_tol;
+    unsigned* bar;               // 64-bit arrival counter (zeroed before each launch)
+    double* part;                // 2 * ncta * 8 partials (double-buffered by phase)
+    DevStatus* status;
+    CgOut* out;
 };
 
 struct PcgDev {
@@ -45,10 +58,12 @@ struct PcgDev {
     const int* halo_idx;
     const unsigned short* lcol;  // per slot: column as an index into its CTA's halo
     int halo_max;                // largest halo (shared-memory sizing)
-    double* part;                // nblocks * 4 partials + 8 totals
-    unsigned* bar;               // [0] count, [1] generation
+    double* part;                // 2 * nblocks * 8 partials (double-buffered by phase)
+    unsigned* bar;               // 64-bit arrival counter
     DevStatus* status;
     CgOut* out;
+    const int* cta_inst;         // batched launch: instance of each CTA (else null)
+    const PcgInst* inst;         // batched launch: instance descriptors (else null)
 };
 
 // Owns the device copies of the pattern and the PCG work vectors.
@@ -108,6 +123,84 @@ public:
     // traffic of the two phases.
     size_t bytes_per_iter() const;
     long long nnz_offdiag = 0;
+};
+
+// ----------------------------------------------------------- batched solves
+// Many independent pressure systems (one per instance of a batch) solved by
+// the same persistent kernels: instances are packed into waves, each wave is
+// one cooperative launch in which every instance owns its own CTAs, halo,
+// reductions, barrier, status and result.
+struct PcgBatchMember {
+    const HostModel* m;
+    const uint8_t* d_nflag;      // the instance's node flags, node order
+    const double* d_pfix;        // fixed-pressure values, node order
+    DevStatus* d_status;         // the instance's status word
+};
+
+// A tiling of the batch: rows per thread (1, 2, 4 or 8 slices of 32 rows per
+// warp) and whether the spare CTAs of a wave are shared out by instance size.
+struct PcgBatchPlan {
+    int rmax = 4;
+    int spread = 1;
+};
+
+class PcgBatch {
+public:
+    void init(const std::vector<PcgBatchMember>& members, int device, bool mixed, double inner_tol);
+    // Builds the waves of a plan; false (with the reason) when it cannot fit.
+    bool plan(const PcgBatchPlan& p, std::string* why);
+    void release();
+    // Instance k, on its own stream: operator values from its state,
+    // constraints, and its inputs moved to row-position order.
+    void prepare(int k, const DevState& S, cudaStream_t st);
+    // Every wave, in order, on one stream.
+    void solve(cudaStream_t st);
+    // Instance k: the pressure back to node order.
+    void finish(int k, double* d_pres, cudaStream_t st);
+    CgOut* out(int k) const { return d_out + k; }
+    int nwaves() const { return static_cast<int>(waves.size()); }
+    // launches per step: assemble, impose, permute in and out per instance; one per wave
+    int launches_per_instance() const { return 4; }
+    PcgBatchPlan current{};
+    bool mixed_any = false;      // some wave runs the mixed-precision kernel
+
+private:
+    struct Wave {
+        int G = 0, rmax = 4;
+        bool mixed = false;
+        size_t smem = 0;
+        const void* fn = nullptr;
+        PcgDev dev{};
+        int* d_cta_inst = nullptr;
+        PcgInst* d_inst = nullptr;
+        int *d_hptr = nullptr, *d_hidx = nullptr;
+    };
+    void free_waves();
+    std::vector<PcgBatchMember> mem;
+    std::vector<int> slice0, nsl, N_k;
+    std::vector<long long> slot0, nslot;
+    std::vector<long long*> d_cptr;
+    std::vector<int*> d_cent;
+    std::vector<Wave> waves;
+    int device = 0, sms = 0, gmax = 0;
+    bool mixed = false;
+    int nslices = 0, NP = 0;
+    long long nslots = 0;
+    std::vector<long long> h_slice_off;
+    std::vector<int> h_col;
+    long long* d_slice_off = nullptr;
+    int *d_slice_w = nullptr, *d_col = nullptr, *d_row_node = nullptr;
+    unsigned short* d_lcol = nullptr;
+    double* d_val = nullptr;
+    float* d_val32 = nullptr;
+    double *d_r = nullptr, *d_z = nullptr, *d_pA = nullptr, *d_pB = nullptr, *d_q = nullptr;
+    double *d_xp = nullptr, *d_bp = nullptr, *d_dp = nullptr;
+    uint8_t* d_fp = nullptr;
+    float* d_f32 = nullptr;
+    double* d_part = nullptr;
+    unsigned* d_bar = nullptr;
+    CgOut* d_out = nullptr;
+    PcgDev base{};
 };
 
 // Launches a grid whose barrier can never complete and reports the status

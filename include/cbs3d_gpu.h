@@ -231,6 +231,53 @@ cbs3d_status cbs3d_convergence_norms_static(int device, const double* unkno, con
                                             const unsigned char* node_flags, int npoin, int temp_calc,
                                             double hb[15]);
 
+/* ---------------------------------------------------------------------------
+ * Batched step (no reference counterpart; each instance is the reference's
+ * single-case step): many independent cases of any sizes advanced together.
+ * Per step, every instance's stages run on its own stream (graph branches);
+ * all pressure systems are solved by one cooperative launch per wave of
+ * instances, each instance with its own reductions, stopping test, status
+ * and result.  The whole step is one CUDA graph when use_graph is set.
+ * --------------------------------------------------------------------------- */
+typedef struct cbs3d_batch cbs3d_batch;
+
+typedef struct cbs3d_batch_options {
+    cbs3d_options base;      /* precision, device, inner_tol, use_graph (pcg_kernel/pcg_blocks unused) */
+    int autotune;            /* 1: on the first step time every feasible PCG tiling on the real
+                                systems and keep the fastest */
+    int rows_per_thread;     /* tiling without autotune: 1, 2, 4 or 8 slices of 32 rows per warp
+                                (0: 4) */
+    int spread;              /* 1: a wave's spare CTAs are shared out by instance size; 0: each
+                                instance gets the fewest CTAs that hold its rows */
+} cbs3d_batch_options;
+
+typedef struct cbs3d_batch_info {
+    int instances;
+    int waves;               /* cooperative PCG launches per step */
+    int rows_per_thread;     /* tiling in use */
+    int spread;
+    int mixed_waves;         /* 1 when a wave runs the mixed-precision kernel */
+    int tuned;               /* 1 after the autotuner ran */
+    int candidates;          /* tilings the autotuner timed */
+    int cand_rows[8], cand_spread[8];
+    double cand_ms[8];       /* one batched pressure solve per candidate, ms (-1: did not fit) */
+} cbs3d_batch_info;
+
+void cbs3d_default_batch_options(cbs3d_batch_options* opt);
+/* n instances, each a mesh and parameter set as for cbs3d_create; all on opt->base.device. */
+cbs3d_status cbs3d_batch_create(int n, const cbs3d_mesh* meshes, const cbs3d_params* params,
+                                const cbs3d_batch_options* opt, cbs3d_batch** out, char* err, size_t errlen);
+/* nsteps steps of every instance.  stats: n entries (or NULL), each as
+ * cbs3d_step returns it for that instance; *gpu_seconds (or NULL): device
+ * time of the whole call (after the autotuned first step, when the
+ * autotuner runs in this call).  A failing instance stops the call after the step
+ * in which it failed; its status and message are returned. */
+cbs3d_status cbs3d_batch_step(cbs3d_batch* b, int nsteps, cbs3d_step_stats* stats, double* gpu_seconds);
+cbs3d_status cbs3d_batch_download_fields(cbs3d_batch* b, int instance, double* u, double* p, double* t);
+cbs3d_status cbs3d_batch_get_info(const cbs3d_batch* b, cbs3d_batch_info* info);
+void cbs3d_batch_destroy(cbs3d_batch* b);
+const char* cbs3d_batch_last_error(const cbs3d_batch* b);
+
 /* Failure-detection self-test (no reference counterpart): launches a small
  * grid whose grid barrier can never complete and returns, in
  * *observed_status, the status its bounded device waits recorded --
