@@ -298,6 +298,29 @@ def cavity_batch(count: int = 48, n_lo: int = 10, n_hi: int = 40, re_lo: float =
     return [cavity(int(n), re=float(r), ntime=ntime, relToler=rel_tol, **over) for n, r in zip(ns, res)]
 
 
+def channel_adjoint(nx: int = 96, ny: int = 16, nz: int = 16, length: float = 6.0, re: float = 100.0,
+                    dtfix: float = 0.01, ntime: int = 200, rel_tol: float = 1.0e-13, **over) -> Case:
+    """Channel for the body-force sensitivities: parabolic inlet (BC 508,
+    u_max 1) at x=0, zero-pressure outlet (520) at x=L, no-slip walls, nu =
+    1/Re, and a fixed time step dtfix (the tangent and adjoint runs need one)."""
+    return channel(nx, ny, nz, length=length, re=re, ntime=ntime, dtfixed=1, dtfix=dtfix, relToler=rel_tol, **over)
+
+
+def region_weights(case: Case, axis: int = 0, lo: float = 4.0, hi: float = 5.0) -> np.ndarray:
+    """Objective weights of a mean over the nodes with lo <= x_axis <= hi:
+    J = 1/2 sum w_i |u_i|^2 is then their mean kinetic energy."""
+    x = case.mesh.coord.reshape(-1, 3)[:, axis]
+    sel = (x >= lo - 1e-12) & (x <= hi + 1e-12)
+    w = np.zeros(case.mesh.npoin)
+    w[sel] = 1.0 / max(int(sel.sum()), 1)
+    return w
+
+
+def body_force(case: Case, sigma: float = 0.01, seed: int = 4321) -> np.ndarray:
+    """Seeded per-node body force, every component ~ N(0, sigma^2), node-major."""
+    return np.random.default_rng(seed).normal(0.0, sigma, size=3 * case.mesh.npoin)
+
+
 def channel(nx: int = 96, ny: int = 16, nz: int = 16, length: float = 6.0, re: float = 100.0,
             ntime: int = 10, symmetry_z: bool = False, **over) -> Case:
     """Channel [0,L]x[0,1]x[0,1]: BC 508 parabolic inlet at x=0, BC 520 outlet

@@ -159,6 +159,10 @@ def lib():
         L.cbs3d_pcg_destroy.argtypes = [vp]
         L.cbs3d_pcg_last_error.argtypes = [vp]
         L.cbs3d_pcg_last_error.restype = cp
+        L.cbs3d_set_body_force.argtypes = [vp, vp]
+        L.cbs3d_objective_run.argtypes = [vp, _i, vp, ctypes.POINTER(_d)]
+        L.cbs3d_tlm_run.argtypes = [vp, _i, vp, vp, ctypes.POINTER(_d), ctypes.POINTER(_d)]
+        L.cbs3d_adjoint_run.argtypes = [vp, _i, _i, vp, ctypes.POINTER(_d), vp]
         L.cbs3d_default_batch_options.argtypes = [ctypes.POINTER(BatchOptions)]
         L.cbs3d_batch_create.argtypes = [_i, ctypes.POINTER(Mesh), ctypes.POINTER(Params),
                                          ctypes.POINTER(BatchOptions), ctypes.POINTER(vp), cp, ctypes.c_size_t]
@@ -173,6 +177,7 @@ def lib():
         for fn in ("cbs3d_create", "cbs3d_create_from_case", "cbs3d_read_params", "cbs3d_step",
                    "cbs3d_upload_fields", "cbs3d_download_fields", "cbs3d_get_array", "cbs3d_set_array",
                    "cbs3d_run_stage", "cbs3d_pressure_multiply", "cbs3d_pcg_create", "cbs3d_pcg_solve",
+                   "cbs3d_set_body_force", "cbs3d_objective_run", "cbs3d_tlm_run", "cbs3d_adjoint_run",
                    "cbs3d_batch_create", "cbs3d_batch_step", "cbs3d_batch_download_fields", "cbs3d_batch_get_info"):
             getattr(L, fn).restype = _i
         _lib = L
@@ -304,6 +309,38 @@ class Context:
     def upload(self, u=None, p=None, t=None):
         arrs = [None if x is None else np.ascontiguousarray(x, dtype=np.float64) for x in (u, p, t)]
         self._check(lib().cbs3d_upload_fields(self.h, *[_ptr(a) for a in arrs]))
+
+    # ---- body force, tangent-linear and adjoint runs (extension)
+    def set_body_force(self, f=None):
+        """f[3*npoin] node-major, or None to remove it."""
+        a = None if f is None else np.ascontiguousarray(f, dtype=np.float64).reshape(-1)
+        if a is not None and a.size != 3 * self.npoin:
+            raise ValueError("body force must have 3*npoin entries")
+        self._bf = a
+        self._check(lib().cbs3d_set_body_force(self.h, _ptr(a)))
+
+    def objective(self, nsteps: int, w) -> float:
+        """J = 1/2 sum w_i |u_i|^2 after nsteps steps; the state is restored."""
+        w = np.ascontiguousarray(w, dtype=np.float64)
+        J = ctypes.c_double()
+        self._check(lib().cbs3d_objective_run(self.h, nsteps, _ptr(w), ctypes.byref(J)))
+        return J.value
+
+    def tlm(self, nsteps: int, w, df):
+        """(J, dJ/df . df) from the tangent-linear model; the state is restored."""
+        w = np.ascontiguousarray(w, dtype=np.float64)
+        df = np.ascontiguousarray(df, dtype=np.float64).reshape(-1)
+        J, dJ = ctypes.c_double(), ctypes.c_double()
+        self._check(lib().cbs3d_tlm_run(self.h, nsteps, _ptr(w), _ptr(df), ctypes.byref(J), ctypes.byref(dJ)))
+        return J.value, dJ.value
+
+    def adjoint(self, nsteps: int, w, every: int = 20):
+        """(J, dJ/df[3*npoin]) with checkpoints every `every` steps; the state is restored."""
+        w = np.ascontiguousarray(w, dtype=np.float64)
+        g = np.empty(3 * self.npoin)
+        J = ctypes.c_double()
+        self._check(lib().cbs3d_adjoint_run(self.h, nsteps, every, _ptr(w), ctypes.byref(J), _ptr(g)))
+        return J.value, g
 
     def pressure_multiply(self, x) -> np.ndarray:
         x = np.ascontiguousarray(x, dtype=np.float64)

@@ -8,6 +8,7 @@
 #include "host_model.h"
 #include "kernels.cuh"
 #include "pcg.cuh"
+#include "ctx.cuh"
 
 #include <cstdio>
 #include <cstring>
@@ -19,14 +20,8 @@
 
 using namespace cbs3d;
 
-#define CUDA_OK(x) do { cudaError_t e_ = (x); if (e_ != cudaSuccess) throw Error(CBS3D_CUDA_ERROR, std::string(#x) + ": " + cudaGetErrorString(e_)); } while (0)
 
 namespace {
-
-constexpr int T = 256;
-constexpr int LOG_FIELDS = 24;   // dtreal, cg[6], hb[15], rtime, spare
-
-inline unsigned nb(long long n, int t = T) { return static_cast<unsigned>((n + t - 1) / t); }
 
 // Records one step: dtreal, the PCG result, hb, rtime; tags a pending failure
 // with the step counter.
@@ -50,7 +45,9 @@ __global__ void k_step_log(DevState S, const CgOut* cg, double* log, int* counte
     r[23] = cg->outer;
 }
 
-std::string reason_text(const DevStatus& s)
+}  // namespace
+
+std::string cbs3d::reason_text(const DevStatus& s)
 {
     const std::string at = std::to_string(s.where);
     switch (s.reason) {
@@ -89,92 +86,10 @@ std::string reason_text(const DevStatus& s)
     }
 }
 
-struct DeviceBuffers {
-    std::vector<void*> ptrs;
-    template <typename Tp>
-    Tp* alloc(size_t n)
-    {
-        void* p = nullptr;
-        CUDA_OK(cudaMalloc(&p, (n ? n : 1) * sizeof(Tp)));
-        ptrs.push_back(p);
-        return static_cast<Tp*>(p);
-    }
-    template <typename Tp>
-    Tp* upload(const std::vector<Tp>& v)
-    {
-        Tp* p = alloc<Tp>(v.size());
-        if (!v.empty()) CUDA_OK(cudaMemcpy(p, v.data(), v.size() * sizeof(Tp), cudaMemcpyHostToDevice));
-        return p;
-    }
-    void release()
-    {
-        for (void* p : ptrs) cudaFree(p);
-        ptrs.clear();
-    }
-};
+namespace {
 
 }  // namespace
 
-struct cbs3d_ctx {
-    HostModel m;
-    cbs3d_options opt{};
-    cudaStream_t st = nullptr;
-    DevState S{};
-    DeviceBuffers buf;
-    int* d_color_elem = nullptr;
-    double* d_log = nullptr;
-    int* d_counter = nullptr;
-    int log_cap = 0;
-    int conv_blocks = 0;
-    PcgEngine pcg;
-    int iitime = 0;
-    long long cg_total = 0;
-    std::string err;
-    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
-    cudaGraphExec_t gexec = nullptr;
-    bool graph_failed = false;
-    std::vector<cudaEvent_t> pcg_ev;   // 2 per step when timing PCG launches
-    int pcg_ev_used = 0;
-    long long launches = 0;            // kernels enqueued (counted at enqueue time)
-    int step_kernels = 0;              // kernels per enqueued step
-    CgOut* batch_out = nullptr;        // member of a batch: its pressure-solve result (no own PCG engine)
-
-    ~cbs3d_ctx()
-    {
-        for (cudaEvent_t e : pcg_ev) cudaEventDestroy(e);
-        if (gexec) cudaGraphExecDestroy(gexec);
-        pcg.release();
-        buf.release();
-        if (ev0) cudaEventDestroy(ev0);
-        if (ev1) cudaEventDestroy(ev1);
-        if (st) cudaStreamDestroy(st);
-    }
-
-    bool fixed_dt(int it) const
-    {
-        // TimeStep::computeTimeStep fixed branch (src/timestep/TimeStep.cpp:492-509)
-        return m.p.ilots <= -1 || m.p.dtfixed > 0 || (m.p.dtfix_end > 0 && it <= m.p.dtfix_end);
-    }
-    bool force_global() const
-    {
-        // src/timestep/TimeStep.cpp:544-547
-        return m.p.transient_on > 0 || m.p.solver_opt > 1 || m.p.dtfixed == -1 ||
-               (m.p.ilots != 1 && m.p.ilots != 2);
-    }
-
-    void setup(bool own_pcg = true);
-    void check_status();
-    void reset_status() { CUDA_OK(cudaMemsetAsync(S.status, 0, sizeof(DevStatus), st)); }
-    void stage_time_step(int it);
-    void stage_solve();
-    // Solver::advanceOneStep in two halves around the pressure solve
-    void enqueue_pre(int it);
-    void enqueue_post(int it);
-    void enqueue_step(int it);
-    // kernels of one step outside the pressure solve
-    int kernels_outside_solve(int it) const;
-    void ensure_log(int n);
-};
 
 void cbs3d_ctx::setup(bool own_pcg)
 {

@@ -71,6 +71,11 @@ struct DevState {
     // fields
     double *unkno, *unkn1, *pres, *pres1, *temp, *temp1, *velocity;
     double *rhs, *rhs1, *delte, *elcoe2, *elcoe2p, *pdiag, *mdiag_real;
+    // body force (extension, no reference counterpart): f[3N] node-major and
+    // the fluid lumped mass mfluid[N]; Step 1 adds mfluid*f to the momentum
+    // residual.  Both null when no body force is set.
+    const double* bforce;
+    const double* mfluid;
     // element-local scratch (12E doubles, reused by every assembly stage)
     double* elbuf;
     // scalars

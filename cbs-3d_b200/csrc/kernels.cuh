@@ -8,6 +8,7 @@ namespace cbs3d {
 __global__ void k_geometry(DevState S);
 __global__ void k_mass(DevState S);
 __global__ void k_nodal_length(DevState S);
+__global__ void k_mass_fluid(DevState S, double* mfluid);
 __global__ void k_begin_step(DevState S);
 __global__ void k_timestep(DevState S, int fixed_dt);
 __global__ void k_dt_finish(DevState S, int fixed_dt);

@@ -144,6 +144,19 @@ __global__ void k_mass(DevState S)
     S.elcoe2p[i] = 1.0 / t;
 }
 
+// Fluid lumped mass per node (element order), for the body-force term.
+__global__ void k_mass_fluid(DevState S, double* mfluid)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= S.P.N) return;
+    double m = 0.0;
+    for (int k = S.n2e_ptr[i]; k < S.n2e_ptr[i + 1]; ++k) {
+        const int e = S.n2e[k] >> 2;
+        if (S.mat[e] == 0) m += S.detJ[e] * MASS_FACTOR;
+    }
+    mfluid[i] = m;
+}
+
 // compute_nodal_lengths_from_elements (src/timestep/TimeStep.cpp:319-355):
 // minimum altitude over the incident tetrahedra (order-independent).
 __global__ void k_nodal_length(DevState S)
@@ -569,6 +582,12 @@ __global__ void k_step1_node(DevState S)
         r0 += S.elbuf[(size_t)(0 * 4 + a) * E + e];
         r1 += S.elbuf[(size_t)(1 * 4 + a) * E + e];
         r2 += S.elbuf[(size_t)(2 * 4 + a) * E + e];
+    }
+    if (S.bforce) {
+        const double mf = S.mfluid[i];
+        r0 += mf * S.bforce[3 * i];
+        r1 += mf * S.bforce[3 * i + 1];
+        r2 += mf * S.bforce[3 * i + 2];
     }
     S.rhs[3 * i] = r0; S.rhs[3 * i + 1] = r1; S.rhs[3 * i + 2] = r2;
     const double m = S.elcoe2[i];

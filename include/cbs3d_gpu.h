@@ -232,6 +232,26 @@ cbs3d_status cbs3d_convergence_norms_static(int device, const double* unkno, con
                                             double hb[15]);
 
 /* ---------------------------------------------------------------------------
+ * Body force, tangent-linear and adjoint runs (no reference counterpart).
+ * A per-node body force f[3*npoin] (node-major) adds M_f f to the Step-1
+ * momentum residual (M_f: fluid lumped mass).  The objective of the runs is
+ * J = 1/2 sum_i w[i] |u_i|^2 after nsteps steps from the context's current
+ * state; every run restores the state (fields, step counter, time) when it
+ * returns.  Tangent and adjoint runs need a fixed time step (dtfixed > 0),
+ * under which the pressure operator is constant; the adjoint's pressure
+ * systems reuse the context's PCG operator.
+ * --------------------------------------------------------------------------- */
+/* f = NULL removes the body force. */
+cbs3d_status cbs3d_set_body_force(cbs3d_ctx* ctx, const double* f);
+/* J only (the forward run of the other two). */
+cbs3d_status cbs3d_objective_run(cbs3d_ctx* ctx, int nsteps, const double* w, double* J);
+/* J and the directional derivative dJ = (dJ/df) . df of the tangent-linear model. */
+cbs3d_status cbs3d_tlm_run(cbs3d_ctx* ctx, int nsteps, const double* w, const double* df, double* J, double* dJ);
+/* J and grad[3*npoin] = dJ/df: forward with (u, p) checkpoints every `every`
+ * steps, then the reverse sweep recomputing one segment at a time. */
+cbs3d_status cbs3d_adjoint_run(cbs3d_ctx* ctx, int nsteps, int every, const double* w, double* J, double* grad);
+
+/* ---------------------------------------------------------------------------
  * Batched step (no reference counterpart; each instance is the reference's
  * single-case step): many independent cases of any sizes advanced together.
  * Per step, every instance's stages run on its own stream (graph branches);

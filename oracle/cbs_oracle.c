@@ -39,6 +39,10 @@ struct orc_state {
     double *dNkdx;   /* 12E: (e*3 + dim)*4 + a */
     double *detJ, *annxf /* 16E: (e*4+face)*4+c */, *face_norm /* 4NB */, *alen_e;
     double *elcoe_e, *mdiag_real, *pdiagE, *gstifE;
+    /* body force (extension, no reference counterpart): f[3N] and the fluid
+     * lumped mass; Step 1 adds mfluid*f to the residual when has_bforce */
+    double *bforce, *mfluid;
+    int has_bforce;
     int *fedge;      /* 4E */
     char *tf, *ts;   /* touches fluid / solid per node */
     int npoin_wall, *wall_list;
@@ -213,6 +217,7 @@ static int mass_matrix(orc_state* s)
 {
     double* thermal = xcalloc((size_t)s->N, sizeof(double));
     memset(s->mdiag_real, 0, sizeof(double) * (size_t)s->N);
+    memset(s->mfluid, 0, sizeof(double) * (size_t)s->N);
     for (int e = 0; e < s->E; ++e) {
         if (s->detJ[e] <= 0.0 || !isfinite(s->detJ[e])) { free(thermal); return fail(s, "Preprocess::massMatrix - invalid detJ at element %d", e + 1); }
         if (s->rho_cp[e] <= 0.0 || !isfinite(s->rho_cp[e])) { free(thermal); return fail(s, "Preprocess::massMatrix - invalid rho*cp at element %d", e + 1); }
@@ -221,6 +226,7 @@ static int mass_matrix(orc_state* s)
         for (int a = 0; a < 4; ++a) {
             const int ip = NODE(s, e, a);
             s->mdiag_real[ip] += nm;
+            if (s->mat[e] == 0) s->mfluid[ip] += nm;
             thermal[ip] += nc;
             s->elcoe_e[(size_t)e * 4 + a] = nm;
         }
@@ -568,6 +574,7 @@ orc_state* orc_create(const orc_params* p, int nelem, int npoin, int nboun,
     s->annxf = xcalloc(16 * E, sizeof(double)); s->face_norm = xcalloc(4 * NB, sizeof(double));
     s->alen_e = xcalloc(E, sizeof(double)); s->elcoe_e = xcalloc(4 * E, sizeof(double));
     s->mdiag_real = xcalloc(N, sizeof(double));
+    s->mfluid = xcalloc(N, sizeof(double)); s->bforce = xcalloc(3 * N, sizeof(double));
     s->pdiagE = xcalloc(4 * E, sizeof(double)); s->gstifE = xcalloc(6 * E, sizeof(double));
     s->fedge = xcalloc(4 * E, sizeof(int));
     s->tf = xcalloc(N, 1); s->ts = xcalloc(N, 1);
@@ -656,7 +663,8 @@ void orc_destroy(orc_state* s)
                     s->elcoe_e, s->mdiag_real, s->pdiagE, s->gstifE, s->fedge, s->tf, s->ts,
                     s->wall_list, s->bc_list, s->bc_values, s->color_ptr, s->color_elem,
                     s->unkno, s->unkn1, s->pres, s->pres1, s->temp, s->temp1, s->velocity,
-                    s->rhs, s->rhs1, s->delte, s->alen, s->elcoe2, s->elcoe2p, s->pdiag, s->gstif};
+                    s->rhs, s->rhs1, s->delte, s->alen, s->elcoe2, s->elcoe2p, s->pdiag, s->gstif,
+                    s->bforce, s->mfluid};
     for (size_t i = 0; i < sizeof ptrs / sizeof ptrs[0]; ++i) free(ptrs[i]);
     free(s);
 }
@@ -946,6 +954,9 @@ int orc_step1(orc_state* s)
             for (int a = 0; a < 4; ++a) for (int i = 0; i < 3; ++i) s->rhs[3 * (size_t)ipn[a] + i] += lrhs[i][a];
         }
     if (bad_detj) return fail(s, "MomentumAssembly::assembleStep1Rhs - invalid detJ at one or more elements");
+    if (s->has_bforce)
+        for (int ip = 0; ip < s->N; ++ip)
+            for (int d = 0; d < 3; ++d) s->rhs[3 * (size_t)ip + d] += s->mfluid[ip] * s->bforce[3 * (size_t)ip + d];
     for (int ip = 0; ip < s->N; ++ip)
         for (int d = 0; d < 3; ++d)
             s->unkno[3 * (size_t)ip + d] = s->unkn1[3 * (size_t)ip + d] + s->rhs[3 * (size_t)ip + d] * s->elcoe2[ip];
@@ -1291,6 +1302,7 @@ static void* lookup(orc_state* s, const char* n, long* count, char* type)
     I("color_ptr", s->color_ptr, s->ncolor + 1) I("color_elem", s->color_elem, E)
     I("bc_list", s->bc_list, s->bc_fixed) D("bc_values", s->bc_values, s->bc_fixed)
     I("wall_node_list", s->wall_list, s->npoin_wall)
+    D("bforce", s->bforce, 3 * N) D("mfluid", s->mfluid, N)
     D("unkno", s->unkno, 3 * N) D("unkn1", s->unkn1, 3 * N) D("pres", s->pres, N)
     D("pres1", s->pres1, N) D("temperature", s->temp, N) D("temperature1", s->temp1, N)
     D("velocity", s->velocity, N) D("rhs", s->rhs, 3 * N) D("rhs1", s->rhs1, N)
@@ -1325,5 +1337,6 @@ int orc_set(orc_state* s, const char* name, const void* in, long count)
     void* p = lookup(s, name, &n, &t);
     if (!p || count != n) return 1;
     memcpy(p, in, (size_t)n * (t == 'd' ? sizeof(double) : sizeof(int)));
+    if (p == (void*)s->bforce) s->has_bforce = 1;
     return 0;
 }
