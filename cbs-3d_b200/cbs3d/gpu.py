@@ -163,6 +163,11 @@ def lib():
         L.cbs3d_objective_run.argtypes = [vp, _i, vp, ctypes.POINTER(_d)]
         L.cbs3d_tlm_run.argtypes = [vp, _i, vp, vp, ctypes.POINTER(_d), ctypes.POINTER(_d)]
         L.cbs3d_adjoint_run.argtypes = [vp, _i, _i, vp, ctypes.POINTER(_d), vp]
+        L.cbs3d_heat_flux_face_count.argtypes = [vp, ctypes.POINTER(_i)]
+        L.cbs3d_set_face_heat_flux.argtypes = [vp, vp]
+        L.cbs3d_heat_objective_run.argtypes = [vp, _i, vp, ctypes.POINTER(_d)]
+        L.cbs3d_heat_tlm_run.argtypes = [vp, _i, vp, vp, ctypes.POINTER(_d), ctypes.POINTER(_d)]
+        L.cbs3d_heat_adjoint_run.argtypes = [vp, _i, _i, vp, ctypes.POINTER(_d), vp]
         L.cbs3d_default_batch_options.argtypes = [ctypes.POINTER(BatchOptions)]
         L.cbs3d_batch_create.argtypes = [_i, ctypes.POINTER(Mesh), ctypes.POINTER(Params),
                                          ctypes.POINTER(BatchOptions), ctypes.POINTER(vp), cp, ctypes.c_size_t]
@@ -178,6 +183,8 @@ def lib():
                    "cbs3d_upload_fields", "cbs3d_download_fields", "cbs3d_get_array", "cbs3d_set_array",
                    "cbs3d_run_stage", "cbs3d_pressure_multiply", "cbs3d_pcg_create", "cbs3d_pcg_solve",
                    "cbs3d_set_body_force", "cbs3d_objective_run", "cbs3d_tlm_run", "cbs3d_adjoint_run",
+                   "cbs3d_heat_flux_face_count", "cbs3d_set_face_heat_flux", "cbs3d_heat_objective_run",
+                   "cbs3d_heat_tlm_run", "cbs3d_heat_adjoint_run",
                    "cbs3d_batch_create", "cbs3d_batch_step", "cbs3d_batch_download_fields", "cbs3d_batch_get_info"):
             getattr(L, fn).restype = _i
         _lib = L
@@ -340,6 +347,39 @@ class Context:
         g = np.empty(3 * self.npoin)
         J = ctypes.c_double()
         self._check(lib().cbs3d_adjoint_run(self.h, nsteps, every, _ptr(w), ctypes.byref(J), _ptr(g)))
+        return J.value, g
+
+    def heat_flux_faces(self) -> int:
+        n = _i()
+        self._check(lib().cbs3d_heat_flux_face_count(self.h, ctypes.byref(n)))
+        return n.value
+
+    def set_face_heat_flux(self, q=None):
+        """Per-face heat flux on the BC-532 faces, or None for the uniform value."""
+        a = None if q is None else np.ascontiguousarray(q, dtype=np.float64)
+        self._q = a
+        self._check(lib().cbs3d_set_face_heat_flux(self.h, _ptr(a)))
+
+    def heat_objective(self, nsteps: int, w) -> float:
+        """J = sum w_i T_i after nsteps steps; the state is restored."""
+        w = np.ascontiguousarray(w, dtype=np.float64)
+        J = ctypes.c_double()
+        self._check(lib().cbs3d_heat_objective_run(self.h, nsteps, _ptr(w), ctypes.byref(J)))
+        return J.value
+
+    def heat_tlm(self, nsteps: int, w, dq):
+        w = np.ascontiguousarray(w, dtype=np.float64)
+        dq = np.ascontiguousarray(dq, dtype=np.float64)
+        J, dJ = ctypes.c_double(), ctypes.c_double()
+        self._check(lib().cbs3d_heat_tlm_run(self.h, nsteps, _ptr(w), _ptr(dq), ctypes.byref(J), ctypes.byref(dJ)))
+        return J.value, dJ.value
+
+    def heat_adjoint(self, nsteps: int, w, every: int = 20):
+        """(J, dJ/dq[faces]) with checkpoints every `every` steps; the state is restored."""
+        w = np.ascontiguousarray(w, dtype=np.float64)
+        g = np.empty(self.heat_flux_faces())
+        J = ctypes.c_double()
+        self._check(lib().cbs3d_heat_adjoint_run(self.h, nsteps, every, _ptr(w), ctypes.byref(J), _ptr(g)))
         return J.value, g
 
     def pressure_multiply(self, x) -> np.ndarray:

@@ -467,6 +467,118 @@ __global__ void k_adj_s1_node(DevState S, const double* u1, const double* rhs_s1
     }
 }
 
+
+// ------------------------------------------------------------- energy step
+// Step-4 element residual as T-coefficients: lr[a] = sum_d c[d][a] t_d with
+// t_d = sum_b g[d][b] T_b (advection, its stabilisation, conduction; the
+// volumetric source does not depend on T).
+__device__ void s4_coef(const DevState& S, int e, double (&g)[3][4], double (&c)[3][4])
+{
+    const int E = S.P.E;
+    const int4 n = S.intma[e];
+    const double det = S.detJ[e], rcp = S.rho_cp[e], k = S.kc[e];
+#pragma unroll
+    for (int d = 0; d < 3; ++d)
+#pragma unroll
+        for (int a = 0; a < 4; ++a) { g[d][a] = S.grad[(size_t)(d * 4 + a) * E + e]; c[d][a] = 0.0; }
+    if (S.mat[e] == 0) {
+        double u[3][4], sum[3] = {0.0, 0.0, 0.0};
+        for (int a = 0; a < 4; ++a)
+            for (int d = 0; d < 3; ++d) { u[d][a] = S.unkno[3 * nd(n, a) + d]; sum[d] += u[d][a]; }
+        const double af = rcp * det / 120.0;
+        for (int a = 0; a < 4; ++a)
+            for (int d = 0; d < 3; ++d) c[d][a] -= af * (sum[d] + u[d][a]);
+        const double tau = 0.5 * S.delte[e] * rcp * (det / 6.0);
+        const double ub[3] = {sum[0] / 4.0, sum[1] / 4.0, sum[2] / 4.0};
+        for (int a = 0; a < 4; ++a) {
+            const double ug = ub[0] * g[0][a] + ub[1] * g[1][a] + ub[2] * g[2][a];
+            for (int d = 0; d < 3; ++d) c[d][a] += tau * ug * ub[d];
+        }
+    }
+    const double kv = k * (det / 6.0);
+    for (int a = 0; a < 4; ++a)
+        for (int d = 0; d < 3; ++d) c[d][a] -= kv * g[d][a];
+}
+
+__global__ void k_tlm_s4_elem(DevState S, const double* dT, double* eb)
+{
+    const int E = S.P.E;
+    const int e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= E) return;
+    const int4 n = S.intma[e];
+    double g[3][4], c[3][4];
+    s4_coef(S, e, g, c);
+    double t[3] = {0.0, 0.0, 0.0};
+    for (int b = 0; b < 4; ++b)
+        for (int d = 0; d < 3; ++d) t[d] += g[d][b] * dT[nd(n, b)];
+    for (int a = 0; a < 4; ++a) eb[(size_t)a * E + e] = c[0][a] * t[0] + c[1][a] * t[1] + c[2][a] * t[2];
+}
+
+// dT^{n+1} = dT^n + m_p (K dT^n + H dq) off the Dirichlet-T nodes, 0 on them
+__global__ void k_tlm_s4_node(DevState S, const double* eb, const int* hf_face, const double* hf_area,
+                              const double* dq, const double* dT, double* dTn)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= S.P.N) return;
+    const int E = S.P.E;
+    double r = 0.0;
+    for (int k = S.n2e_ptr[i]; k < S.n2e_ptr[i + 1]; ++k) {
+        const int e = S.n2e[k] >> 2, a = S.n2e[k] & 3;
+        r += eb[(size_t)a * E + e];
+    }
+    if (dq)
+        for (int k = S.hf_ptr[i]; k < S.hf_ptr[i + 1]; ++k) r += dq[hf_face[k]] * hf_area[k] / 3.0;
+    dTn[i] = S.tbc_flag[i] ? 0.0 : dT[i] + r * S.elcoe2p[i];
+}
+
+__global__ void k_adj_s4_node(DevState S, const double* lam, double* lpre, double* mu)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= S.P.N) return;
+    const double l = S.tbc_flag[i] ? 0.0 : lam[i];
+    lpre[i] = l;
+    mu[i] = S.elcoe2p[i] * l;
+}
+
+__global__ void k_adj_s4_elem(DevState S, const double* mu, double* eb)
+{
+    const int E = S.P.E;
+    const int e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= E) return;
+    const int4 n = S.intma[e];
+    double g[3][4], c[3][4];
+    s4_coef(S, e, g, c);
+    double s[3] = {0.0, 0.0, 0.0};
+    for (int a = 0; a < 4; ++a) {
+        const double m = mu[nd(n, a)];
+        for (int d = 0; d < 3; ++d) s[d] += m * c[d][a];
+    }
+    for (int b = 0; b < 4; ++b) eb[(size_t)b * E + e] = g[0][b] * s[0] + g[1][b] * s[1] + g[2][b] * s[2];
+}
+
+// lam^n = lpre + K^T mu (every element, element order)
+__global__ void k_adj_s4_gather(DevState S, const double* eb, const double* lpre, double* lam)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= S.P.N) return;
+    const int E = S.P.E;
+    double r = lpre[i];
+    for (int k = S.n2e_ptr[i]; k < S.n2e_ptr[i + 1]; ++k) {
+        const int e = S.n2e[k] >> 2, a = S.n2e[k] & 3;
+        r += eb[(size_t)a * E + e];
+    }
+    lam[i] = r;
+}
+
+// dJ/dq_f += area_f/3 * sum of mu over the face's nodes
+__global__ void k_adj_qface(int nqf, const int* qf_nodes, const double* qf_area, const double* mu, double* grad)
+{
+    const int f = blockIdx.x * blockDim.x + threadIdx.x;
+    if (f >= nqf) return;
+    const double s = mu[qf_nodes[3 * f]] + mu[qf_nodes[3 * f + 1]] + mu[qf_nodes[3 * f + 2]];
+    grad[f] += qf_area[f] / 3.0 * s;
+}
+
 // ------------------------------------------------------------------ driver
 // Work space of one tangent or adjoint run on a context; the context's
 // fields, step counter and physical time are restored when it ends.
@@ -583,6 +695,65 @@ public:
         CUDA_OK(cudaMemcpyAsync(v0, v3, 3 * N * sizeof(double), cudaMemcpyDeviceToDevice, st));
         CUDA_OK(cudaGetLastError());
     }
+    // heat-flux face data on the device (once per run)
+    void heat_setup()
+    {
+        if (c.m.qf_area.empty())
+            throw Error(CBS3D_INVALID_INPUT, "heat-flux runs need BC-532 faces and heat_flux_bc != 0 in the case");
+        nqf = static_cast<int>(c.m.qf_area.size());
+        hf_face = reinterpret_cast<int*>(alloc((c.m.hf_face.size() + 1) / 2 + 1));
+        hf_area = alloc(c.m.hf_area.size());
+        qf_nodes = reinterpret_cast<int*>(alloc((c.m.qf_nodes.size() + 1) / 2 + 1));
+        qf_area = alloc(c.m.qf_area.size());
+        CUDA_OK(cudaMemcpy(hf_face, c.m.hf_face.data(), c.m.hf_face.size() * sizeof(int), cudaMemcpyHostToDevice));
+        CUDA_OK(cudaMemcpy(hf_area, c.m.hf_area.data(), c.m.hf_area.size() * sizeof(double), cudaMemcpyHostToDevice));
+        CUDA_OK(cudaMemcpy(qf_nodes, c.m.qf_nodes.data(), c.m.qf_nodes.size() * sizeof(int), cudaMemcpyHostToDevice));
+        CUDA_OK(cudaMemcpy(qf_area, c.m.qf_area.data(), c.m.qf_area.size() * sizeof(double), cudaMemcpyHostToDevice));
+    }
+    // energy tangent step after forward(): s0 = dT^n in, dT^{n+1} out
+    void heat_tangent(const double* dq)
+    {
+        const unsigned gn = nb(static_cast<long long>(N)), ge = nb(static_cast<long long>(E));
+        k_tlm_s4_elem<<<ge, T, 0, st>>>(c.S, s0, eb12);
+        k_tlm_s4_node<<<gn, T, 0, st>>>(c.S, eb12, hf_face, hf_area, dq, s0, s1);
+        CUDA_OK(cudaMemcpyAsync(s0, s1, N * sizeof(double), cudaMemcpyDeviceToDevice, st));
+        CUDA_OK(cudaGetLastError());
+    }
+    // energy adjoint step after forward(): s0 = adjoint of T^{n+1} in, of T^n out
+    void heat_adjoint(double* grad)
+    {
+        const unsigned gn = nb(static_cast<long long>(N)), ge = nb(static_cast<long long>(E));
+        k_adj_s4_node<<<gn, T, 0, st>>>(c.S, s0, s1, pd);
+        k_adj_qface<<<nb(nqf), T, 0, st>>>(nqf, qf_nodes, qf_area, pd, grad);
+        k_adj_s4_elem<<<ge, T, 0, st>>>(c.S, pd, eb12);
+        k_adj_s4_gather<<<gn, T, 0, st>>>(c.S, eb12, s1, s0);
+        CUDA_OK(cudaGetLastError());
+    }
+    // J = sum_i w_i T_i; optionally its gradient w into s0
+    double objective_T(const double* w, bool seed)
+    {
+        std::vector<double> t(N);
+        CUDA_OK(cudaMemcpyAsync(t.data(), c.S.temp, N * sizeof(double), cudaMemcpyDeviceToHost, st));
+        CUDA_OK(cudaStreamSynchronize(st));
+        c.check_status();
+        double J = 0.0;
+        for (size_t i = 0; i < N; ++i) J += w[i] * t[i];
+        if (seed) {
+            CUDA_OK(cudaMemcpyAsync(s0, w, N * sizeof(double), cudaMemcpyHostToDevice, st));
+            CUDA_OK(cudaStreamSynchronize(st));
+        }
+        return J;
+    }
+    double dot_plain(const double* w, const double* dvec)
+    {
+        std::vector<double> d(N);
+        CUDA_OK(cudaMemcpyAsync(d.data(), dvec, N * sizeof(double), cudaMemcpyDeviceToHost, st));
+        CUDA_OK(cudaStreamSynchronize(st));
+        double s = 0.0;
+        for (size_t i = 0; i < N; ++i) s += w[i] * d[i];
+        return s;
+    }
+
     // J = 1/2 sum_i w_i |u_i|^2 of the current u; optionally lambda_N = w u into v0
     double objective(const double* w, bool seed)
     {
@@ -630,7 +801,55 @@ public:
     int it0 = 0, time_pcg0 = 0;
     PcgEngine pcg;
     bool pcg_ready = false;
+    int nqf = 0;
+    int *hf_face = nullptr, *qf_nodes = nullptr;
+    double *hf_area = nullptr, *qf_area = nullptr;
 };
+
+// Forward sweep with (u, p, T) checkpoints every `every` steps, then the
+// reverse sweep one segment at a time: for each step in reverse the state
+// before it is restored, the step is recomputed (step(true) captures what
+// the adjoint step linearises about) and back(s) runs the adjoint step.
+template <typename Back>
+void reverse_sweep(Run& r, cbs3d_ctx* c, int nsteps, int every, Back&& back)
+{
+    const size_t N = r.N;
+    const int ncp = (nsteps + every - 1) / every;
+    const int seg = every < nsteps ? every : nsteps;
+    std::vector<double*> cp(static_cast<size_t>(ncp)), sg(static_cast<size_t>(seg));
+    for (auto& p : cp) p = r.alloc(5 * N);
+    for (auto& p : sg) p = r.alloc(5 * N);
+    auto save = [&](double* b) {
+        CUDA_OK(cudaMemcpyAsync(b, c->S.unkno, 3 * N * sizeof(double), cudaMemcpyDeviceToDevice, r.st));
+        CUDA_OK(cudaMemcpyAsync(b + 3 * N, c->S.pres, N * sizeof(double), cudaMemcpyDeviceToDevice, r.st));
+        CUDA_OK(cudaMemcpyAsync(b + 4 * N, c->S.temp, N * sizeof(double), cudaMemcpyDeviceToDevice, r.st));
+    };
+    auto load = [&](const double* b) {
+        CUDA_OK(cudaMemcpyAsync(c->S.unkno, b, 3 * N * sizeof(double), cudaMemcpyDeviceToDevice, r.st));
+        CUDA_OK(cudaMemcpyAsync(c->S.pres, b + 3 * N, N * sizeof(double), cudaMemcpyDeviceToDevice, r.st));
+        CUDA_OK(cudaMemcpyAsync(c->S.temp, b + 4 * N, N * sizeof(double), cudaMemcpyDeviceToDevice, r.st));
+    };
+    for (int s = 0; s < nsteps; ++s) {
+        if (s % every == 0) save(cp[static_cast<size_t>(s / every)]);
+        r.forward(false);
+    }
+    back(-1);   // seed at the final state
+    for (int k = ncp - 1; k >= 0; --k) {
+        const int a = k * every, b = (a + every < nsteps) ? a + every : nsteps;
+        load(cp[static_cast<size_t>(k)]);
+        c->iitime = r.it0 + a;
+        for (int s = a; s < b; ++s) {
+            save(sg[static_cast<size_t>(s - a)]);
+            r.forward(false);
+        }
+        for (int s = b - 1; s >= a; --s) {
+            load(sg[static_cast<size_t>(s - a)]);
+            c->iitime = r.it0 + s;
+            r.forward(true);
+            back(s);
+        }
+    }
+}
 
 template <typename F>
 cbs3d_status run_guarded(cbs3d_ctx* c, F&& f)
@@ -715,45 +934,88 @@ cbs3d_status cbs3d_adjoint_run(cbs3d_ctx* c, int nsteps, int every, const double
         Run r(*c);
         r.check_fixed_dt(nsteps);
         const size_t N = r.N;
-        const int ncp = (nsteps + every - 1) / every;
-        std::vector<double*> cpu(static_cast<size_t>(ncp)), cpp(static_cast<size_t>(ncp));
-        for (int k = 0; k < ncp; ++k) { cpu[static_cast<size_t>(k)] = r.alloc(3 * N); cpp[static_cast<size_t>(k)] = r.alloc(N); }
-        const int seg = every < nsteps ? every : nsteps;
-        std::vector<double*> sgu(static_cast<size_t>(seg)), sgp(static_cast<size_t>(seg));
-        for (int k = 0; k < seg; ++k) { sgu[static_cast<size_t>(k)] = r.alloc(3 * N); sgp[static_cast<size_t>(k)] = r.alloc(N); }
         double* G = r.alloc(3 * N);
         CUDA_OK(cudaMemsetAsync(G, 0, 3 * N * sizeof(double), r.st));
-        auto save = [&](double* du, double* dp) {
-            CUDA_OK(cudaMemcpyAsync(du, c->S.unkno, 3 * N * sizeof(double), cudaMemcpyDeviceToDevice, r.st));
-            CUDA_OK(cudaMemcpyAsync(dp, c->S.pres, N * sizeof(double), cudaMemcpyDeviceToDevice, r.st));
-        };
-        auto load = [&](const double* du, const double* dp) {
-            CUDA_OK(cudaMemcpyAsync(c->S.unkno, du, 3 * N * sizeof(double), cudaMemcpyDeviceToDevice, r.st));
-            CUDA_OK(cudaMemcpyAsync(c->S.pres, dp, N * sizeof(double), cudaMemcpyDeviceToDevice, r.st));
-        };
-        // forward sweep with checkpoints of (u, p) every `every` steps
-        for (int s = 0; s < nsteps; ++s) {
-            if (s % every == 0) save(cpu[static_cast<size_t>(s / every)], cpp[static_cast<size_t>(s / every)]);
-            r.forward(false);
-        }
-        *J = r.objective(w, true);   // seeds v0 = dJ/du^N
-        // reverse sweep, one checkpoint segment at a time
-        for (int k = ncp - 1; k >= 0; --k) {
-            const int a = k * every, b = (a + every < nsteps) ? a + every : nsteps;
-            load(cpu[static_cast<size_t>(k)], cpp[static_cast<size_t>(k)]);
-            c->iitime = r.it0 + a;
-            for (int s = a; s < b; ++s) {
-                save(sgu[static_cast<size_t>(s - a)], sgp[static_cast<size_t>(s - a)]);
-                r.forward(false);
-            }
-            for (int s = b - 1; s >= a; --s) {
-                load(sgu[static_cast<size_t>(s - a)], sgp[static_cast<size_t>(s - a)]);
-                c->iitime = r.it0 + s;
-                r.forward(true);
-                r.adjoint(G);
-            }
-        }
+        reverse_sweep(r, c, nsteps, every, [&](int s) {
+            if (s < 0) *J = r.objective(w, true);   // v0 = dJ/du^N
+            else r.adjoint(G);
+        });
         CUDA_OK(cudaMemcpyAsync(grad, G, 3 * N * sizeof(double), cudaMemcpyDeviceToHost, r.st));
+        CUDA_OK(cudaStreamSynchronize(r.st));
+        c->check_status();
+        r.restore();
+    });
+}
+
+cbs3d_status cbs3d_heat_flux_face_count(cbs3d_ctx* c, int* nfaces)
+{
+    if (!c || !nfaces) return CBS3D_INVALID_INPUT;
+    *nfaces = static_cast<int>(c->m.qf_area.size());
+    return CBS3D_OK;
+}
+
+cbs3d_status cbs3d_set_face_heat_flux(cbs3d_ctx* c, const double* q)
+{
+    return run_guarded(c, [&] {
+        const HostModel& m = c->m;
+        if (m.qf_area.empty())
+            throw Error(CBS3D_INVALID_INPUT, "cbs3d_set_face_heat_flux - the case has no heat-flux faces (BC 532 with heat_flux_bc != 0)");
+        std::vector<double> v(m.hf_val);
+        if (q)
+            for (size_t k = 0; k < v.size(); ++k) v[k] = q[m.hf_face[k]] * m.hf_area[k] / 3.0;
+        CUDA_OK(cudaMemcpyAsync(const_cast<double*>(c->S.hf_val), v.data(), v.size() * sizeof(double),
+                                cudaMemcpyHostToDevice, c->st));
+        CUDA_OK(cudaStreamSynchronize(c->st));
+    });
+}
+
+cbs3d_status cbs3d_heat_objective_run(cbs3d_ctx* c, int nsteps, const double* w, double* J)
+{
+    return run_guarded(c, [&] {
+        if (nsteps < 1 || !w || !J) throw Error(CBS3D_INVALID_INPUT, "cbs3d_heat_objective_run - nsteps >= 1, w and J required");
+        if (c->m.temp_calc < 1) throw Error(CBS3D_INVALID_INPUT, "cbs3d_heat_objective_run - the case does not solve the energy equation");
+        Run r(*c);
+        for (int s = 0; s < nsteps; ++s) r.forward(false);
+        *J = r.objective_T(w, false);
+        r.restore();
+    });
+}
+
+cbs3d_status cbs3d_heat_tlm_run(cbs3d_ctx* c, int nsteps, const double* w, const double* dq, double* J, double* dJ)
+{
+    return run_guarded(c, [&] {
+        if (nsteps < 1 || !w || !dq || !J || !dJ) throw Error(CBS3D_INVALID_INPUT, "cbs3d_heat_tlm_run - nsteps >= 1, w, dq, J and dJ required");
+        if (c->m.temp_calc < 1) throw Error(CBS3D_INVALID_INPUT, "cbs3d_heat_tlm_run - the case does not solve the energy equation");
+        Run r(*c);
+        r.heat_setup();
+        double* ddq = r.alloc(static_cast<size_t>(r.nqf));
+        CUDA_OK(cudaMemcpyAsync(ddq, dq, static_cast<size_t>(r.nqf) * sizeof(double), cudaMemcpyHostToDevice, r.st));
+        CUDA_OK(cudaMemsetAsync(r.s0, 0, r.N * sizeof(double), r.st));
+        for (int s = 0; s < nsteps; ++s) {
+            r.forward(false);
+            r.heat_tangent(ddq);
+        }
+        *J = r.objective_T(w, false);
+        *dJ = r.dot_plain(w, r.s0);
+        r.restore();
+    });
+}
+
+cbs3d_status cbs3d_heat_adjoint_run(cbs3d_ctx* c, int nsteps, int every, const double* w, double* J, double* grad)
+{
+    return run_guarded(c, [&] {
+        if (nsteps < 1 || every < 1 || !w || !J || !grad)
+            throw Error(CBS3D_INVALID_INPUT, "cbs3d_heat_adjoint_run - nsteps >= 1, every >= 1, w, J and grad required");
+        if (c->m.temp_calc < 1) throw Error(CBS3D_INVALID_INPUT, "cbs3d_heat_adjoint_run - the case does not solve the energy equation");
+        Run r(*c);
+        r.heat_setup();
+        double* G = r.alloc(static_cast<size_t>(r.nqf));
+        CUDA_OK(cudaMemsetAsync(G, 0, static_cast<size_t>(r.nqf) * sizeof(double), r.st));
+        reverse_sweep(r, c, nsteps, every, [&](int s) {
+            if (s < 0) *J = r.objective_T(w, true);   // s0 = dJ/dT^N
+            else r.heat_adjoint(G);
+        });
+        CUDA_OK(cudaMemcpyAsync(grad, G, static_cast<size_t>(r.nqf) * sizeof(double), cudaMemcpyDeviceToHost, r.st));
         CUDA_OK(cudaStreamSynchronize(r.st));
         c->check_status();
         r.restore();

@@ -945,19 +945,33 @@ void HostModel::build()
         }
     }
     {
-        std::vector<std::vector<double>> hf(Ns);
+        std::vector<std::vector<double>> hf(Ns), ha(Ns);
+        std::vector<std::vector<int>> hfc(Ns);
+        qf_nodes.clear();
+        qf_area.clear();
         if (P.heat_flux_bc != 0.0)
             for (size_t ib = 0; ib < NBs; ++ib) {
                 const int* r = &iside[6 * ib];
                 if (r[5] != 532) continue;
                 const double area = face_norm[4 * ib + 3];
                 const double contrib = P.heat_flux_bc * area / 3.0;
-                for (int k = 0; k < 3; ++k) hf[static_cast<size_t>(r[k] - 1)].push_back(contrib);
+                const int f = static_cast<int>(qf_area.size());
+                for (int k = 0; k < 3; ++k) {
+                    hf[static_cast<size_t>(r[k] - 1)].push_back(contrib);
+                    hfc[static_cast<size_t>(r[k] - 1)].push_back(f);
+                    ha[static_cast<size_t>(r[k] - 1)].push_back(area);
+                    qf_nodes.push_back(r[k] - 1);
+                }
+                qf_area.push_back(area);
             }
         hf_ptr.assign(Ns + 1, 0);
         hf_val.clear();
+        hf_face.clear();
+        hf_area.clear();
         for (size_t i = 0; i < Ns; ++i) {
             for (double v : hf[i]) hf_val.push_back(v);
+            for (int f : hfc[i]) hf_face.push_back(f);
+            for (double a : ha[i]) hf_area.push_back(a);
             hf_ptr[i + 1] = static_cast<int>(hf_val.size());
         }
     }

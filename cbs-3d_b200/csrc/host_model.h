@@ -80,6 +80,12 @@ struct HostModel {
     std::vector<double> tbc_val;     // N
     std::vector<int> hf_ptr;         // N+1
     std::vector<double> hf_val;      // heat-flux face contributions, face order
+    // Heat-flux faces (BC 532, present when heat_flux_bc != 0), for per-face
+    // flux control: each hf_val entry's face and area, and each face's nodes.
+    std::vector<int> hf_face;        // per hf_val entry: face index 0..nqf-1
+    std::vector<double> hf_area;     // per hf_val entry: face area
+    std::vector<int> qf_nodes;       // 3 per face, 0-based
+    std::vector<double> qf_area;     // per face: area
 
     PressurePattern pat;
 

@@ -251,6 +251,18 @@ cbs3d_status cbs3d_tlm_run(cbs3d_ctx* ctx, int nsteps, const double* w, const do
  * steps, then the reverse sweep recomputing one segment at a time. */
 cbs3d_status cbs3d_adjoint_run(cbs3d_ctx* ctx, int nsteps, int every, const double* w, double* J, double* grad);
 
+/* Per-face heat flux (BC 532 faces in the order of the boundary-face list,
+ * present when the case has heat_flux_bc != 0) and its sensitivities: the
+ * objective is J = sum_i w[i] T_i after nsteps steps.  The temperature does
+ * not act on the flow, so J is linear in the fluxes and these runs need no
+ * fixed time step.  q = NULL restores the uniform heat_flux_bc. */
+cbs3d_status cbs3d_heat_flux_face_count(cbs3d_ctx* ctx, int* nfaces);
+cbs3d_status cbs3d_set_face_heat_flux(cbs3d_ctx* ctx, const double* q);
+cbs3d_status cbs3d_heat_objective_run(cbs3d_ctx* ctx, int nsteps, const double* w, double* J);
+cbs3d_status cbs3d_heat_tlm_run(cbs3d_ctx* ctx, int nsteps, const double* w, const double* dq, double* J, double* dJ);
+/* grad[nfaces] = dJ/dq_f, checkpoints every `every` steps. */
+cbs3d_status cbs3d_heat_adjoint_run(cbs3d_ctx* ctx, int nsteps, int every, const double* w, double* J, double* grad);
+
 /* ---------------------------------------------------------------------------
  * Batched step (no reference counterpart; each instance is the reference's
  * single-case step): many independent cases of any sizes advanced together.
