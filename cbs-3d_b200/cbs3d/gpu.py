@@ -79,7 +79,7 @@ class Mesh(ctypes.Structure):
 
 class Options(ctypes.Structure):
     _fields_ = [("precision", _i), ("device", _i), ("inner_tol", _d), ("use_graph", _i),
-                ("pcg_blocks", _i), ("verbose", _i), ("time_pcg", _i), ("pcg_kernel", _i)]
+                ("pcg_blocks", _i), ("verbose", _i), ("time_pcg", _i), ("pcg_kernel", _i), ("case_cache", _i)]
 
 
 class CGResult(ctypes.Structure):
@@ -159,6 +159,9 @@ def lib():
         L.cbs3d_pcg_destroy.argtypes = [vp]
         L.cbs3d_pcg_last_error.argtypes = [vp]
         L.cbs3d_pcg_last_error.restype = cp
+        L.cbs3d_case_digest.argtypes = [cp, _i, ctypes.POINTER(ctypes.c_ulonglong), ctypes.POINTER(_i), cp,
+                                        ctypes.c_size_t]
+        L.cbs3d_case_digest.restype = _i
         L.cbs3d_set_body_force.argtypes = [vp, vp]
         L.cbs3d_objective_run.argtypes = [vp, _i, vp, ctypes.POINTER(_d)]
         L.cbs3d_tlm_run.argtypes = [vp, _i, vp, vp, ctypes.POINTER(_d), ctypes.POINTER(_d)]
@@ -209,6 +212,17 @@ def make_params(p: dict) -> Params:
     return s
 
 
+def case_digest(case_name: str, use_cache: bool = False):
+    """(digest, from_cache) of a case's parsed inputs -- host only, no GPU."""
+    d, hit = ctypes.c_ulonglong(), _i()
+    err = ctypes.create_string_buffer(1024)
+    rc = lib().cbs3d_case_digest(case_name.encode(), 1 if use_cache else 0, ctypes.byref(d), ctypes.byref(hit),
+                                 err, 1024)
+    if rc != 0:
+        raise CBSError(rc, err.value.decode())
+    return d.value, bool(hit.value)
+
+
 def make_options(precision: int = FP64, device: int = 0, inner_tol: float = 1e-5, use_graph: bool = True,
                  pcg_blocks: int = 0, time_pcg: bool = False, pcg_kernel: int = 0) -> Options:
     o = Options()
@@ -252,12 +266,13 @@ class Context:
 
     def __init__(self, case=None, case_name: str | None = None, precision: int = FP64, device: int = 0,
                  inner_tol: float = 1e-5, use_graph: bool = True, pcg_blocks: int = 0, time_pcg: bool = False,
-                 pcg_kernel: int = 0):
+                 pcg_kernel: int = 0, case_cache: bool = False):
         L = lib()
         self.h = ctypes.c_void_p()
         self.device = device
         err = ctypes.create_string_buffer(1024)
         opt = make_options(precision, device, inner_tol, use_graph, pcg_blocks, time_pcg, pcg_kernel)
+        opt.case_cache = 1 if case_cache else 0
         if case_name is not None:
             rc = L.cbs3d_create_from_case(case_name.encode(), ctypes.byref(opt), ctypes.byref(self.h), err, 1024)
         else:

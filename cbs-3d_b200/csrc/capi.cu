@@ -373,6 +373,41 @@ cbs3d_status cbs3d_read_params(const char* case_name, cbs3d_params* params, int*
     }
 }
 
+static void fnv_bytes(unsigned long long* h, const void* data, size_t n)
+{
+    const unsigned char* p = static_cast<const unsigned char*>(data);
+    for (size_t i = 0; i < n; ++i) { *h ^= p[i]; *h *= 1099511628211ULL; }
+}
+#define FNV(h, v) fnv_bytes(&(h), (v).data(), (v).size() * sizeof((v)[0]))
+
+cbs3d_status cbs3d_case_digest(const char* case_name, int use_cache, unsigned long long* digest,
+                               int* from_cache, char* err, size_t errlen)
+{
+    if (!case_name || !digest) return CBS3D_INVALID_INPUT;
+    try {
+        HostModel m;
+        bool hit = false;
+        if (use_cache) hit = parse_case_cached(case_name, m);
+        else parse_case(case_name, m);
+        unsigned long long h = 1469598103934665603ULL;
+        const std::vector<int> sizes = {m.E, m.N, m.NB};
+        FNV(h, sizes); FNV(h, m.intma); FNV(h, m.coord); FNV(h, m.iside); FNV(h, m.mat);
+        FNV(h, m.rho); FNV(h, m.cp); FNV(h, m.kc); FNV(h, m.mu); FNV(h, m.qvol);
+        fnv_bytes(&h, &m.p, sizeof m.p);
+        *digest = h;
+        if (from_cache) *from_cache = hit ? 1 : 0;
+        return CBS3D_OK;
+    } catch (const Error& e) {
+        fill_err(err, errlen, e.what());
+        return e.code;
+    } catch (const std::exception& e) {
+        fill_err(err, errlen, e.what());
+        return CBS3D_INTERNAL;
+    }
+}
+
+#undef FNV
+
 static cbs3d_status create_common(std::unique_ptr<cbs3d_ctx>& c, const cbs3d_options* opt, cbs3d_ctx** out,
                                   char* err, size_t errlen)
 {
@@ -397,7 +432,7 @@ cbs3d_status cbs3d_create_from_case(const char* case_name, const cbs3d_options* 
     *out = nullptr;
     auto c = std::make_unique<cbs3d_ctx>();
     try {
-        read_case(case_name, c->m);
+        read_case(case_name, c->m, opt && opt->case_cache > 0);
     } catch (const Error& e) {
         fill_err(err, errlen, e.what());
         return e.code;

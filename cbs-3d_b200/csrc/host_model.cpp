@@ -13,6 +13,8 @@
 #include <sstream>
 #include <unordered_map>
 
+#include <sys/stat.h>
+
 namespace cbs3d {
 
 namespace {
@@ -327,7 +329,123 @@ void read_params_only(const std::string& case_name, cbs3d_params& p, int& nelem,
 
 // MeshIO::readAll, src/io/MeshIO.cpp:572-609 (readSizes :613-709,
 // readMeshFile :713-868, readBoundaryFile :872-982, materials :1441-1623)
-void read_case(const std::string& case_name, HostModel& m)
+namespace {
+
+// ------------------------------------------------------------- case cache
+// The parsed inputs of a case (sizes, parameters, connectivity, coordinates,
+// boundary faces, material ids and properties) in one binary file beside the
+// case files, keyed by the size and modification time of every source file.
+// Parsing the ASCII mesh dominates set-up for large cases; the cache skips it.
+constexpr char CACHE_MAGIC[16] = "CBS3D-CASE-v1";
+
+struct SourceStamp {
+    long long size = -1, mtime_ns = -1;
+};
+
+SourceStamp stamp(const std::string& path)
+{
+    SourceStamp s;
+    struct stat st;
+    if (::stat(path.c_str(), &st) == 0) {
+        s.size = static_cast<long long>(st.st_size);
+        s.mtime_ns = static_cast<long long>(st.st_mtim.tv_sec) * 1000000000LL + st.st_mtim.tv_nsec;
+    }
+    return s;
+}
+
+std::vector<SourceStamp> case_stamps(const std::string& c)
+{
+    return {stamp(c + ".plt"), stamp(c + ".bco"), stamp(c + ".par"), stamp(c + ".material"), stamp(c + ".matprop")};
+}
+
+template <typename T>
+void put(std::ofstream& o, const std::vector<T>& v)
+{
+    const unsigned long long n = v.size();
+    o.write(reinterpret_cast<const char*>(&n), sizeof n);
+    if (n) o.write(reinterpret_cast<const char*>(v.data()), static_cast<std::streamsize>(n * sizeof(T)));
+}
+
+template <typename T>
+bool get(std::ifstream& in, std::vector<T>& v, unsigned long long limit)
+{
+    unsigned long long n = 0;
+    if (!in.read(reinterpret_cast<char*>(&n), sizeof n) || n > limit) return false;
+    v.resize(static_cast<size_t>(n));
+    if (n) in.read(reinterpret_cast<char*>(v.data()), static_cast<std::streamsize>(n * sizeof(T)));
+    return static_cast<bool>(in);
+}
+
+bool load_cache(const std::string& case_name, HostModel& m)
+{
+    std::ifstream in(case_name + ".cbscache", std::ios::binary);
+    if (!in) return false;
+    char magic[16] = {};
+    in.read(magic, sizeof magic);
+    if (!in || std::memcmp(magic, CACHE_MAGIC, sizeof magic) != 0) return false;
+    unsigned long long psize = 0;
+    in.read(reinterpret_cast<char*>(&psize), sizeof psize);
+    if (!in || psize != sizeof(cbs3d_params)) return false;
+    std::vector<SourceStamp> st(5);
+    in.read(reinterpret_cast<char*>(st.data()), static_cast<std::streamsize>(st.size() * sizeof(SourceStamp)));
+    const std::vector<SourceStamp> now = case_stamps(case_name);
+    for (size_t i = 0; i < st.size(); ++i)
+        if (!in || st[i].size != now[i].size || st[i].mtime_ns != now[i].mtime_ns) return false;
+    in.read(reinterpret_cast<char*>(&m.p), sizeof m.p);
+    int sizes[3] = {0, 0, 0};
+    in.read(reinterpret_cast<char*>(sizes), sizeof sizes);
+    if (!in || sizes[0] < 1 || sizes[1] < 1 || sizes[2] < 0) return false;
+    m.E = sizes[0]; m.N = sizes[1]; m.NB = sizes[2];
+    const unsigned long long lim = 1ULL << 40;
+    return get(in, m.intma, lim) && get(in, m.coord, lim) && get(in, m.iside, lim) && get(in, m.mat, lim) &&
+           get(in, m.rho, lim) && get(in, m.cp, lim) && get(in, m.kc, lim) && get(in, m.mu, lim) &&
+           get(in, m.rho_cp, lim) && get(in, m.alpha, lim) && get(in, m.qvol, lim) &&
+           m.intma.size() == 4 * static_cast<size_t>(m.E) && m.coord.size() == 3 * static_cast<size_t>(m.N) &&
+           m.iside.size() == 6 * static_cast<size_t>(m.NB) && m.mat.size() == static_cast<size_t>(m.E);
+}
+
+void save_cache(const std::string& case_name, const HostModel& m)
+{
+    const std::string path = case_name + ".cbscache";
+    const std::string tmp = path + ".tmp";
+    {
+        std::ofstream o(tmp, std::ios::binary | std::ios::trunc);
+        if (!o) return;   // read-only case directory: no cache
+        o.write(CACHE_MAGIC, sizeof CACHE_MAGIC);
+        const unsigned long long psize = sizeof(cbs3d_params);
+        o.write(reinterpret_cast<const char*>(&psize), sizeof psize);
+        const std::vector<SourceStamp> st = case_stamps(case_name);
+        o.write(reinterpret_cast<const char*>(st.data()), static_cast<std::streamsize>(st.size() * sizeof(SourceStamp)));
+        o.write(reinterpret_cast<const char*>(&m.p), sizeof m.p);
+        const int sizes[3] = {m.E, m.N, m.NB};
+        o.write(reinterpret_cast<const char*>(sizes), sizeof sizes);
+        put(o, m.intma); put(o, m.coord); put(o, m.iside); put(o, m.mat);
+        put(o, m.rho); put(o, m.cp); put(o, m.kc); put(o, m.mu); put(o, m.rho_cp); put(o, m.alpha); put(o, m.qvol);
+        if (!o) { std::remove(tmp.c_str()); return; }
+    }
+    std::rename(tmp.c_str(), path.c_str());
+}
+
+}  // namespace
+
+bool parse_case_cached(const std::string& case_name, HostModel& m)
+{
+    if (load_cache(case_name, m)) return true;
+    parse_case(case_name, m);
+    save_cache(case_name, m);
+    return false;
+}
+
+void read_case(const std::string& case_name, HostModel& m, bool use_cache, bool* from_cache)
+{
+    bool hit = false;
+    if (use_cache) hit = parse_case_cached(case_name, m);
+    else parse_case(case_name, m);
+    if (from_cache) *from_cache = hit;
+    m.build();
+}
+
+void parse_case(const std::string& case_name, HostModel& m)
 {
     cbs3d_params& p = m.p;
     default_params(p);
@@ -470,7 +588,6 @@ void read_case(const std::string& case_name, HostModel& m)
             m.alpha[e] = m.kc[e] / m.rho_cp[e];
         }
     }
-    m.build();
 }
 
 void model_from_arrays(const cbs3d_mesh& mesh, const cbs3d_params& p, HostModel& m)

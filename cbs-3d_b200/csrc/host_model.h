@@ -95,7 +95,13 @@ struct HostModel {
 };
 
 // Parses the case files with the grammar of MeshIO::readAll.
-void read_case(const std::string& case_name, HostModel& m);
+// Parses and builds; with use_cache the parsed inputs are taken from (or
+// written to) <case>.cbscache when every source file's size and time match.
+void read_case(const std::string& case_name, HostModel& m, bool use_cache = false, bool* from_cache = nullptr);
+// The parse alone (the model's inputs; build() not run), and the same through
+// the cache (returns true when the inputs came from it).
+void parse_case(const std::string& case_name, HostModel& m);
+bool parse_case_cached(const std::string& case_name, HostModel& m);
 void read_params_only(const std::string& case_name, cbs3d_params& p, int& nelem, int& npoin,
                       int& nboun);
 // Fills the model from in-memory arrays (raw ids already mapped).

@@ -97,6 +97,8 @@ typedef struct cbs3d_options {
     int time_pcg;            /* time every PCG launch with CUDA events (no graph capture) */
     int pcg_kernel;          /* 0 automatic; 1 vectors in global memory, 2 register-resident rows,
                                 3 shared-memory halo, 4 halo + one grid sync per iteration */
+    int case_cache;          /* cbs3d_create_from_case: keep the parsed case in <case>.cbscache
+                                (keyed by every source file's size and time) and reuse it */
 } cbs3d_options;
 
 /* Mirrors ConjugateGradient::Result (include/cbs/linalg/ConjugateGradient.hpp:36-68).
@@ -145,6 +147,13 @@ void cbs3d_default_params(cbs3d_params* p);
  * sizes and parameters.  Replaces MeshIO::readSizes/readParameterFile. */
 cbs3d_status cbs3d_read_params(const char* case_name, cbs3d_params* params,
                                int* nelem, int* npoin, int* nboun, char* err, size_t errlen);
+
+/* Host only (no device; no reference counterpart): parses <case> as
+ * cbs3d_create_from_case does, through the binary cache when use_cache, and
+ * returns a 64-bit digest of the parsed inputs and whether they came from
+ * the cache. */
+cbs3d_status cbs3d_case_digest(const char* case_name, int use_cache, unsigned long long* digest,
+                               int* from_cache, char* err, size_t errlen);
 
 /* Reads the case files and builds a device context: replaces MeshIO::readAll
  * + Solver::initialise + Solver::preparePressureSystem

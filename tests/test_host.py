@@ -81,3 +81,32 @@ def test_fixture_case_roundtrip():
     case, z = load_case(fixture_path("cht"))
     assert case.params["temp_calc"] == 1
     assert case.mesh.nelem == int(z["ref_sizes"][0])
+
+
+def test_case_cache_round_trip(tmp_path):
+    """The binary case cache returns exactly the parsed inputs, is reused
+    while the source files are unchanged and is rebuilt when one changes."""
+    import time
+    from cbs3d import cases, gpu
+    c = cases.cht_slab(6, 3, 2, 2, ntime=5)
+    base = c.write(str(tmp_path), "cht")
+    ref, hit = gpu.case_digest(base)
+    assert not hit
+    d1, hit1 = gpu.case_digest(base, use_cache=True)
+    assert (d1, hit1) == (ref, False) and os.path.exists(base + ".cbscache")
+    d2, hit2 = gpu.case_digest(base, use_cache=True)
+    assert (d2, hit2) == (ref, True)
+    time.sleep(0.01)
+    with open(base + ".par", "a") as f:
+        f.write("\n")
+    d3, hit3 = gpu.case_digest(base, use_cache=True)
+    assert not hit3 and d3 == ref
+
+
+def test_case_cache_faster_on_large_mesh(tmp_path):
+    import time
+    from cbs3d import cases, gpu
+    base = cases.cavity(28, ntime=5).write(str(tmp_path), "cav")
+    t0 = time.perf_counter(); gpu.case_digest(base, use_cache=True); t_parse = time.perf_counter() - t0
+    t0 = time.perf_counter(); _, hit = gpu.case_digest(base, use_cache=True); t_cache = time.perf_counter() - t0
+    assert hit and t_cache < 0.5 * t_parse
