@@ -162,6 +162,14 @@ def lib():
         L.cbs3d_case_digest.argtypes = [cp, _i, ctypes.POINTER(ctypes.c_ulonglong), ctypes.POINTER(_i), cp,
                                         ctypes.c_size_t]
         L.cbs3d_case_digest.restype = _i
+        L.cbs3d_write_vtu_case.argtypes = [cp, cp, vp, vp, vp, cp, ctypes.c_size_t]
+        L.cbs3d_write_vtu_case.restype = _i
+        L.cbs3d_write_vtu.argtypes = [vp, cp]
+        L.cbs3d_write_vtu.restype = _i
+        L.cbs3d_write_residual_rows.argtypes = [vp, cp, _i]
+        L.cbs3d_write_residual_rows.restype = _i
+        L.cbs3d_step_history.argtypes = [vp, _i, _i, vp]
+        L.cbs3d_step_history.restype = _i
         L.cbs3d_set_body_force.argtypes = [vp, vp]
         L.cbs3d_objective_run.argtypes = [vp, _i, vp, ctypes.POINTER(_d)]
         L.cbs3d_tlm_run.argtypes = [vp, _i, vp, vp, ctypes.POINTER(_d), ctypes.POINTER(_d)]

@@ -9,6 +9,7 @@
 #include "kernels.cuh"
 #include "pcg.cuh"
 #include "ctx.cuh"
+#include "post.h"
 
 #include <cstdio>
 #include <cstring>
@@ -577,6 +578,8 @@ cbs3d_status cbs3d_step(cbs3d_ctx* c, int nsteps, int stop_on_steady, cbs3d_step
         CUDA_OK(cudaStreamSynchronize(c->st));
         float ms = 0.0f;
         cudaEventElapsedTime(&ms, c->ev0, c->ev1);
+        c->last_start = start;
+        c->last_done = done;
         const DevStatus s = collect_call(c, done, start, launches0, steady, ms, stats);
         if (s.code != 0) {
             const int fstep = start + (s.step > 0 ? s.step : done);
@@ -1246,5 +1249,80 @@ cbs3d_status cbs3d_batch_get_info(const cbs3d_batch* b, cbs3d_batch_info* info)
 void cbs3d_batch_destroy(cbs3d_batch* b) { delete b; }
 
 const char* cbs3d_batch_last_error(const cbs3d_batch* b) { return b ? b->err.c_str() : "null batch"; }
+
+
+// ----------------------------------------------------------------- output
+cbs3d_status cbs3d_step_history(cbs3d_ctx* c, int first, int count, double* rec)
+{
+    return guarded(c, [&] {
+        if (!rec || first < 0 || count < 0 || first + count > c->last_done)
+            throw Error(CBS3D_INVALID_INPUT, "cbs3d_step_history - range outside the latest call's steps");
+        if (count) CUDA_OK(cudaMemcpy(rec, c->d_log + static_cast<size_t>(first) * LOG_FIELDS,
+                                      static_cast<size_t>(count) * LOG_FIELDS * sizeof(double), cudaMemcpyDeviceToHost));
+    });
+}
+
+cbs3d_status cbs3d_write_residual_rows(cbs3d_ctx* c, const char* path, int header)
+{
+    return guarded(c, [&] {
+        if (!path) throw Error(CBS3D_INVALID_INPUT, "cbs3d_write_residual_rows - path required");
+        if (c->m.p.residual_log_enabled < 1) return;
+        if (header) write_residual_header(path);
+        const int n = c->last_done;
+        if (n < 1) return;
+        std::vector<double> rec(static_cast<size_t>(n) * LOG_FIELDS);
+        CUDA_OK(cudaMemcpy(rec.data(), c->d_log, rec.size() * sizeof(double), cudaMemcpyDeviceToHost));
+        append_residual_rows(path, c->last_start + 1, c->m.p.residual_log_every, rec.data(), n);
+    });
+}
+
+cbs3d_status cbs3d_write_vtu(cbs3d_ctx* c, const char* path)
+{
+    return guarded(c, [&] {
+        if (!path) throw Error(CBS3D_INVALID_INPUT, "cbs3d_write_vtu - path required");
+        const size_t N = c->m.N;
+        std::vector<double> u(3 * N), p(N), t(N), v(N);
+        CUDA_OK(cudaStreamSynchronize(c->st));
+        CUDA_OK(cudaMemcpy(u.data(), c->S.unkno, 3 * N * sizeof(double), cudaMemcpyDeviceToHost));
+        CUDA_OK(cudaMemcpy(p.data(), c->S.pres, N * sizeof(double), cudaMemcpyDeviceToHost));
+        CUDA_OK(cudaMemcpy(t.data(), c->S.temp, N * sizeof(double), cudaMemcpyDeviceToHost));
+        CUDA_OK(cudaMemcpy(v.data(), c->S.velocity, N * sizeof(double), cudaMemcpyDeviceToHost));
+        // before the first step the device magnitude is not yet computed
+        write_vtu(path, c->m, u.data(), p.data(), t.data(), c->iitime > 0 ? v.data() : nullptr);
+    });
+}
+
+cbs3d_status cbs3d_write_vtu_case(const char* case_name, const char* path, const double* u, const double* p,
+                                  const double* t, char* err, size_t errlen)
+{
+    if (!case_name || !path || !u || !p || !t) return CBS3D_INVALID_INPUT;
+    try {
+        HostModel m;
+        parse_case(case_name, m);
+        write_vtu(path, m, u, p, t, nullptr);
+        return CBS3D_OK;
+    } catch (const Error& e) {
+        fill_err(err, errlen, e.what());
+        return e.code;
+    } catch (const std::exception& e) {
+        fill_err(err, errlen, e.what());
+        return CBS3D_INTERNAL;
+    }
+}
+
+cbs3d_status cbs3d_write_pvd(const char* path, int n, const char* const* files, const double* times)
+{
+    if (!path || n < 0 || (n > 0 && (!files || !times))) return CBS3D_INVALID_INPUT;
+    try {
+        std::vector<std::string> f;
+        for (int i = 0; i < n; ++i) f.emplace_back(files[i]);
+        write_pvd(path, f, std::vector<double>(times, times + n));
+        return CBS3D_OK;
+    } catch (const Error& e) {
+        return e.code;
+    } catch (const std::exception&) {
+        return CBS3D_INTERNAL;
+    }
+}
 
 }  // extern "C"

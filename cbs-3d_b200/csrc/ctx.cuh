@@ -76,6 +76,7 @@ struct cbs3d_ctx {
     long long launches = 0;            // kernels enqueued (counted at enqueue time)
     int step_kernels = 0;              // kernels per enqueued step
     CgOut* batch_out = nullptr;        // member of a batch: its pressure-solve result (no own PCG engine)
+    int last_start = 0, last_done = 0; // step counter before, and steps of, the latest cbs3d_step call
     double* d_bforce = nullptr;        // body force f[3N] (extension), when set
     double* d_mfluid = nullptr;        // fluid lumped mass, for the body force
 

@@ -200,6 +200,27 @@ cbs3d_status cbs3d_run_stage(cbs3d_ctx* ctx, const char* stage);
 cbs3d_status cbs3d_pressure_multiply(cbs3d_ctx* ctx, const double* x, double* y);
 
 /* ---------------------------------------------------------------------------
+ * Run output (Post::writeResidualRow / writeVTU / writePVD,
+ * reference src/io/Post.cpp:525-560, 768-815, 887-1180).  Residual rows come
+ * from the device step log of the latest cbs3d_step call (dtreal, the PCG
+ * result, the 15 Convergence::evaluate measures, time), so no field leaves
+ * the device for them.  VTU files are binary-appended with the reference's
+ * arrays and cells (tets, then boundary triangles).
+ * --------------------------------------------------------------------------- */
+/* Records of steps [first, first+count) of the latest cbs3d_step call, 24
+ * doubles each: dtreal, cg iterations, initial_l2, final_l2, relative_l2,
+ * max_abs, converged, hb[15], rtime, outer sweeps. */
+cbs3d_status cbs3d_step_history(cbs3d_ctx* ctx, int first, int count, double* records);
+/* Appends the latest call's rows to the residual CSV (header first when
+ * header != 0), honouring residual_log_enabled / residual_log_every. */
+cbs3d_status cbs3d_write_residual_rows(cbs3d_ctx* ctx, const char* path, int header);
+cbs3d_status cbs3d_write_vtu(cbs3d_ctx* ctx, const char* path);
+/* Host only: the VTU of a case's mesh with caller fields (u[3N], p[N], t[N]). */
+cbs3d_status cbs3d_write_vtu_case(const char* case_name, const char* path, const double* u, const double* p,
+                                  const double* t, char* err, size_t errlen);
+cbs3d_status cbs3d_write_pvd(const char* path, int n, const char* const* files, const double* times);
+
+/* ---------------------------------------------------------------------------
  * Pressure-solver drop-in: a solver_opt backend with the inputs and side
  * effects of ConjugateGradient::solvePressure(CBSStateSI&)
  * (reference src/linalg/ConjugateGradient.cpp:584-869; dispatch at

@@ -42,3 +42,22 @@ def stage_step(z) -> int:
 
 def params_of(case) -> dict:
     return case.params
+
+
+def read_vtu(path):
+    """Arrays of a binary-appended (raw, UInt64 headers) VTU file by name;
+    the points under 'Points'."""
+    import re
+    raw = open(path, "rb").read()
+    head, _, rest = raw.partition(b"<AppendedData encoding=\"raw\">")
+    data = rest[rest.index(b"_") + 1:]
+    types = {"Float64": np.float64, "Int32": np.int32, "UInt8": np.uint8}
+    out = {}
+    for m in re.finditer(rb'<DataArray type="(\w+)"(?: Name="(\w+)")? NumberOfComponents="(\d+)" format="appended" offset="(\d+)"/>', head):
+        t, name, nc, off = m.group(1).decode(), m.group(2), int(m.group(3)), int(m.group(4))
+        n = int(np.frombuffer(data[off:off + 8], dtype=np.uint64)[0])
+        a = np.frombuffer(data[off + 8:off + 8 + n], dtype=types[t])
+        out[name.decode() if name else "Points"] = a.reshape(-1, nc) if nc > 1 else a
+    cells = re.search(rb'NumberOfPoints="(\d+)" NumberOfCells="(\d+)"', head)
+    out["_npoints"], out["_ncells"] = int(cells.group(1)), int(cells.group(2))
+    return out

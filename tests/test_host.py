@@ -110,3 +110,40 @@ def test_case_cache_faster_on_large_mesh(tmp_path):
     t0 = time.perf_counter(); gpu.case_digest(base, use_cache=True); t_parse = time.perf_counter() - t0
     t0 = time.perf_counter(); _, hit = gpu.case_digest(base, use_cache=True); t_cache = time.perf_counter() - t0
     assert hit and t_cache < 0.5 * t_parse
+
+
+def test_vtu_writer_layout(tmp_path):
+    """The VTU carries the reference writer's arrays and cells: tets then
+    boundary triangles, masks from the element materials, masked fields."""
+    from cbs3d import cases, gpu
+    from helpers import read_vtu
+    c = cases.cht_slab(4, 2, 2, 2, ntime=3)
+    base = c.write(str(tmp_path), "cht")
+    N, E, NB = c.mesh.npoin, c.mesh.nelem, c.mesh.nboun
+    rng = np.random.default_rng(0)
+    u, p, t = rng.normal(size=3 * N), rng.normal(size=N), rng.normal(size=N)
+    path = str(tmp_path / "x.vtu")
+    err = ctypes.create_string_buffer(512)
+    rc = gpu.lib().cbs3d_write_vtu_case(base.encode(), path.encode(), gpu._ptr(u), gpu._ptr(p), gpu._ptr(t), err, 512)
+    assert rc == 0, err.value
+    v = read_vtu(path)
+    assert v["_npoints"] == N and v["_ncells"] == E + NB
+    assert np.array_equal(v["Points"].reshape(-1), c.mesh.coord.reshape(-1))
+    conn = v["connectivity"]
+    assert np.array_equal(conn[:4 * E], (c.mesh.intma - 1).reshape(-1))
+    assert np.array_equal(conn[4 * E:], (c.mesh.bfaces[:, :3] - 1).reshape(-1))
+    assert np.array_equal(v["types"], np.r_[np.full(E, 10), np.full(NB, 5)])
+    assert v["offsets"][-1] == 4 * E + 3 * NB
+    mat = c.mesh.mat_elem
+    tf = np.zeros(N, bool); ts = np.zeros(N, bool)
+    for e in range(E):
+        (tf if mat[e] == 0 else ts)[c.mesh.intma[e] - 1] = True
+    assert np.array_equal(v["pressure_active"], tf.astype(np.int32))
+    assert np.array_equal(v["velocity_active"], (tf & ~ts).astype(np.int32))
+    assert np.array_equal(v["node_domain_kind"], np.where(tf & ts, 3, np.where(tf, 1, np.where(ts, 2, 0))))
+    assert np.array_equal(v["pressure"], np.where(tf, p, 0.0))
+    assert np.array_equal(v["temperature"], t)
+    assert np.array_equal(v["velocity"], np.where((tf & ~ts)[:, None], u.reshape(-1, 3), 0.0))
+    assert np.array_equal(v["mat_id"], np.r_[mat, np.full(NB, -1)])
+    assert np.array_equal(v["cell_kind"], np.r_[np.full(E, 1), np.full(NB, 2)])
+    assert np.array_equal(v["parent_element"][:E], np.arange(1, E + 1))
