@@ -32,7 +32,11 @@ namespace cbs3d {
 
 namespace {
 
-constexpr int PCG_THREADS = 256;
+// One 512-thread CTA per SM (128 registers per thread fill the register
+// file): half the CTAs of two 256-thread CTAs per SM, so the grid-wide
+// all-reduce reads half the partials.
+constexpr int PCG_THREADS = 512;
+constexpr int PCG_CTAS_PER_SM = 1;
 constexpr int PCG_WARPS = PCG_THREADS / 32;
 
 #define CUDA_OK(x) do { cudaError_t e_ = (x); if (e_ != cudaSuccess) throw Error(CBS3D_CUDA_ERROR, std::string(#x) + ": " + cudaGetErrorString(e_)); } while (0)
@@ -189,7 +193,7 @@ struct Acc4 {
 
 // Grid-wide all-reduce of (sum a, sum b, max mx, max flag) fused with the
 // grid barrier (grid_allreduce_v below).
-template <int NV, int NSUM>
+template <int NV, int NSUM, int NT = PCG_THREADS>
 __device__ __forceinline__ bool grid_allreduce_v(double (&v)[NV], const PcgDev& D, const SegView& g, int phase,
                                                  double (&out)[NV]);
 
@@ -223,7 +227,7 @@ __device__ __forceinline__ void cg_finish(const PcgDev& D, const SegView& g, int
 }
 
 // ---------------------------------------------------- persistent FP64 PCG
-__global__ void __launch_bounds__(PCG_THREADS) k_pcg64(PcgDev D)
+__global__ void __launch_bounds__(PCG_THREADS, PCG_CTAS_PER_SM) k_pcg64(PcgDev D)
 {
     const SegView g = seg_view<false>(D);
     const int G = g.G, b = g.b;
@@ -356,7 +360,7 @@ __global__ void __launch_bounds__(PCG_THREADS) k_pcg64(PcgDev D)
 // pressure to global memory.  Each row's pair entries are fetched eight at a time before
 // the neighbour gathers are issued, so a lane keeps many loads in flight.
 template <int RMAX>
-__global__ void __launch_bounds__(PCG_THREADS, 2) k_pcg64r(PcgDev D)
+__global__ void __launch_bounds__(PCG_THREADS, PCG_CTAS_PER_SM) k_pcg64r(PcgDev D)
 {
     const SegView g = seg_view<false>(D);
     const int G = g.G, b = g.b;
@@ -535,7 +539,7 @@ __global__ void __launch_bounds__(PCG_THREADS, 2) k_pcg64r(PcgDev D)
 // reads only the streamed coefficients from global memory.  The local column
 // indices stay in shared memory for the whole solve.
 template <int RMAX>
-__global__ void __launch_bounds__(PCG_THREADS, 2) k_pcg64h(PcgDev D)
+__global__ void __launch_bounds__(PCG_THREADS, PCG_CTAS_PER_SM) k_pcg64h(PcgDev D)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const SegView g = seg_view<false>(D);
@@ -728,12 +732,12 @@ struct Acc6 {
 // a second round trip through a last-arriving CTA.  The caller passes the
 // number of all-reduces this launch has completed as `phase`.  Returns false
 // when the wait gave up (status TIMEOUT) or another CTA raised a status.
-template <int NV, int NSUM>
+template <int NV, int NSUM, int NT>
 __device__ __forceinline__ bool grid_allreduce_v(double (&v)[NV], const PcgDev& D, const SegView& g, int phase,
                                                  double (&out)[NV])
 {
     static_assert(NV <= 8, "partials hold 8 doubles per CTA");
-    __shared__ double sm[PCG_WARPS][NV];
+    __shared__ double sm[(NT / 32)][NV];
     __shared__ int s_ok;
     const int G = g.G;
     DevStatus* status = seg_status(D, g);
@@ -755,7 +759,7 @@ __device__ __forceinline__ bool grid_allreduce_v(double (&v)[NV], const PcgDev& 
         double t[NV];
 #pragma unroll
         for (int q = 0; q < NV; ++q) t[q] = 0.0;
-        for (int k = 0; k < PCG_WARPS; ++k)
+        for (int k = 0; k < (NT / 32); ++k)
 #pragma unroll
             for (int q = 0; q < NV; ++q) t[q] = q < NSUM ? t[q] + sm[k][q] : fmax(t[q], sm[k][q]);
         double* p = part + (size_t)g.b * 8;
@@ -788,7 +792,7 @@ __device__ __forceinline__ bool grid_allreduce_v(double (&v)[NV], const PcgDev& 
 #pragma unroll
     for (int q = 0; q < NV; ++q) t[q] = 0.0;
     if (ok) {
-        for (int k = threadIdx.x; k < G; k += PCG_THREADS) {
+        for (int k = threadIdx.x; k < G; k += NT) {
             const double* p = part + (size_t)k * 8;
 #pragma unroll
             for (int q = 0; q < NV; ++q) t[q] = q < NSUM ? t[q] + __ldcg(p + q) : fmax(t[q], __ldcg(p + q));
@@ -808,17 +812,18 @@ __device__ __forceinline__ bool grid_allreduce_v(double (&v)[NV], const PcgDev& 
     __syncthreads();
 #pragma unroll
     for (int q = 0; q < NV; ++q) out[q] = 0.0;
-    for (int k = 0; k < PCG_WARPS; ++k)
+    for (int k = 0; k < (NT / 32); ++k)
 #pragma unroll
         for (int q = 0; q < NV; ++q) out[q] = q < NSUM ? out[q] + sm[k][q] : fmax(out[q], sm[k][q]);
     __syncthreads();
     return ok;
 }
 
+template <int NT>
 __device__ __forceinline__ bool grid_allreduce3(Acc6 v, const PcgDev& D, const SegView& g, int phase, Acc6& out)
 {
     double a[5] = {v.a, v.b, v.c, v.mx, v.flag}, o[5];
-    const bool ok = grid_allreduce_v<5, 3>(a, D, g, phase, o);
+    const bool ok = grid_allreduce_v<5, 3, NT>(a, D, g, phase, o);
     out = Acc6{o[0], o[1], o[2], o[3], o[4]};
     return ok;
 }
@@ -828,16 +833,17 @@ struct Acc8 {
     double a, b, c, d, e, mx, flag;
 };
 
+template <int NT>
 __device__ __forceinline__ bool grid_allreduce5(Acc8 v, const PcgDev& D, const SegView& g, int phase, Acc8& out)
 {
     double a[7] = {v.a, v.b, v.c, v.d, v.e, v.mx, v.flag}, o[7];
-    const bool ok = grid_allreduce_v<7, 5>(a, D, g, phase, o);
+    const bool ok = grid_allreduce_v<7, 5, NT>(a, D, g, phase, o);
     out = Acc8{o[0], o[1], o[2], o[3], o[4], o[5], o[6]};
     return ok;
 }
 
-template <int RMAX, bool BATCH>
-__global__ void __launch_bounds__(PCG_THREADS, 2) k_pcg64c(PcgDev D)
+template <int RMAX, bool BATCH, int NT>
+__global__ void __launch_bounds__(NT, NT >= 512 ? 1 : 2) k_pcg64c(PcgDev D)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const SegView g = seg_view<BATCH>(D);
@@ -853,8 +859,8 @@ __global__ void __launch_bounds__(PCG_THREADS, 2) k_pcg64c(PcgDev D)
     double* dzh = vh + D.halo_max;
     int* hidx = reinterpret_cast<int*>(dzh + D.halo_max);
     unsigned short* lcs = reinterpret_cast<unsigned short*>(hidx + D.halo_max);
-    for (int k = threadIdx.x; k < nh; k += PCG_THREADS) hidx[k] = D.halo_idx[h0 + k];
-    for (int k = threadIdx.x; k < nsl; k += PCG_THREADS) lcs[k] = D.lcol[S0 + k];
+    for (int k = threadIdx.x; k < nh; k += NT) hidx[k] = D.halo_idx[h0 + k];
+    for (int k = threadIdx.x; k < nsl; k += NT) lcs[k] = D.lcol[S0 + k];
     int phase = 0;
     const int N = D.N;
     // parity buffers: r in r/pA, w in q/pB, s in z/dz(+N)... laid out by the engine
@@ -869,7 +875,7 @@ __global__ void __launch_bounds__(PCG_THREADS, 2) k_pcg64c(PcgDev D)
     int wmax = 0;
 #pragma unroll
     for (int k = 0; k < RMAX; ++k) {
-        const int sl = s_beg + warp + PCG_WARPS * k;
+        const int sl = s_beg + warp + (NT / 32) * k;
         row[k] = (sl < s_end) ? sl * 32 + lane : -1;
         lbase[k] = 0;
         wr[k] = 0;
@@ -906,16 +912,16 @@ __global__ void __launch_bounds__(PCG_THREADS, 2) k_pcg64c(PcgDev D)
     // ---- phase 0a: r0 = b - A x0 (constraints as the reference), dz
     double off[RMAX];
     __syncthreads();
-    for (int k0 = threadIdx.x; k0 < nh; k0 += 4 * PCG_THREADS) {
+    for (int k0 = threadIdx.x; k0 < nh; k0 += 4 * NT) {
         double a[4];
 #pragma unroll
         for (int u = 0; u < 4; ++u) {
-            const int k = k0 + u * PCG_THREADS;
+            const int k = k0 + u * NT;
             a[u] = __ldcg(D.pres + (k < nh ? hidx[k] : 0));
         }
 #pragma unroll
         for (int u = 0; u < 4; ++u)
-            if (k0 + u * PCG_THREADS < nh) vh[k0 + u * PCG_THREADS] = a[u];
+            if (k0 + u * NT < nh) vh[k0 + u * NT] = a[u];
     }
     __syncthreads();
     offdiag_all(off);
@@ -948,7 +954,7 @@ __global__ void __launch_bounds__(PCG_THREADS, 2) k_pcg64c(PcgDev D)
         sb[0][i] = 0.0;
     }
     Acc6 t{0.0, 0.0, 0.0, 0.0, 0.0};
-    if (!grid_allreduce3(acc, D, g, phase, t)) return;
+    if (!grid_allreduce3<NT>(acc, D, g, phase, t)) return;
     ++phase;
     const double init = sqrt(t.c);
     if (init <= 1.0e-300) { cg_finish(D, g, 0, 1, init, init, 0.0, t.mx); return; }
@@ -958,18 +964,18 @@ __global__ void __launch_bounds__(PCG_THREADS, 2) k_pcg64c(PcgDev D)
 
     // ---- phase 0b: z0 = M^-1 r0, w0 = A z0, gamma0 = (r0,z0), delta0 = (z0,w0)
     __syncthreads();
-    for (int k0 = threadIdx.x; k0 < nh; k0 += 4 * PCG_THREADS) {
+    for (int k0 = threadIdx.x; k0 < nh; k0 += 4 * NT) {
         double a[4], c[4];
 #pragma unroll
         for (int u = 0; u < 4; ++u) {
-            const int k = k0 + u * PCG_THREADS;
+            const int k = k0 + u * NT;
             const int j = k < nh ? hidx[k] : 0;
             a[u] = __ldcg(dz + j);
             c[u] = __ldcg(rb[0] + j);
         }
 #pragma unroll
         for (int u = 0; u < 4; ++u) {
-            const int k = k0 + u * PCG_THREADS;
+            const int k = k0 + u * NT;
             if (k < nh) { dzh[k] = a[u]; vh[k] = c[u] / a[u]; }
         }
     }
@@ -989,7 +995,7 @@ __global__ void __launch_bounds__(PCG_THREADS, 2) k_pcg64c(PcgDev D)
         }
     }
     t = Acc6{0.0, 0.0, 0.0, 0.0, 0.0};
-    if (!grid_allreduce3(acc, D, g, phase, t)) return;
+    if (!grid_allreduce3<NT>(acc, D, g, phase, t)) return;
     ++phase;
     double gam = t.a;
     if (gam <= 1.0e-300 || !isfinite(gam)) { if (b == 0 && threadIdx.x == 0) set_status(seg_status(D, g), 3, ST_PCG, 0, R_PCG_RZ0); return; }
@@ -1008,11 +1014,11 @@ __global__ void __launch_bounds__(PCG_THREADS, 2) k_pcg64c(PcgDev D)
             const double* so = sb[po];
             const double* wo = wb[po];
             const double* ro = rb[po];
-            for (int k0 = threadIdx.x; k0 < nh; k0 += SU * PCG_THREADS) {
+            for (int k0 = threadIdx.x; k0 < nh; k0 += SU * NT) {
                 double a[SU], c[SU], e[SU];
 #pragma unroll
                 for (int u = 0; u < SU; ++u) {
-                    const int k = k0 + u * PCG_THREADS;
+                    const int k = k0 + u * NT;
                     const int j = k < nh ? hidx[k] : 0;
                     a[u] = __ldcg(so + j);
                     c[u] = __ldcg(wo + j);
@@ -1020,7 +1026,7 @@ __global__ void __launch_bounds__(PCG_THREADS, 2) k_pcg64c(PcgDev D)
                 }
 #pragma unroll
                 for (int u = 0; u < SU; ++u) {
-                    const int k = k0 + u * PCG_THREADS;
+                    const int k = k0 + u * NT;
                     if (k < nh) {
                         const double sj = fma(beta, a[u], c[u]);
                         const double rj = fma(-alpha, sj, e[u]);
@@ -1061,7 +1067,7 @@ __global__ void __launch_bounds__(PCG_THREADS, 2) k_pcg64c(PcgDev D)
             }
         }
         t = Acc6{0.0, 0.0, 0.0, 0.0, 0.0};
-        if (!grid_allreduce3(a6, D, g, phase, t)) return;
+        if (!grid_allreduce3<NT>(a6, D, g, phase, t)) return;
         ++phase;
         fin = sqrt(t.c);
         mx = t.mx;
@@ -1097,8 +1103,8 @@ __global__ void __launch_bounds__(PCG_THREADS, 2) k_pcg64c(PcgDev D)
 constexpr double RU_FACTOR = 0.05;
 constexpr int RU_STALL = 256;   // iterations without a correction before one is forced
 
-template <int RMAX, bool BATCH>
-__global__ void __launch_bounds__(PCG_THREADS, 2) k_pcg32m(PcgDev D)
+template <int RMAX, bool BATCH, int NT>
+__global__ void __launch_bounds__(NT, NT >= 512 ? 1 : 2) k_pcg32m(PcgDev D)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const SegView g = seg_view<BATCH>(D);
@@ -1118,8 +1124,8 @@ __global__ void __launch_bounds__(PCG_THREADS, 2) k_pcg32m(PcgDev D)
     int* hidx = reinterpret_cast<int*>(dzh + HM);                       // HM
     float* val32s = reinterpret_cast<float*>(hidx + HM);                // nsl
     unsigned short* lcs = reinterpret_cast<unsigned short*>(val32s + D.slot_max);
-    for (int k = threadIdx.x; k < nh; k += PCG_THREADS) hidx[k] = D.halo_idx[h0 + k];
-    for (int k = threadIdx.x; k < nsl; k += PCG_THREADS) {
+    for (int k = threadIdx.x; k < nh; k += NT) hidx[k] = D.halo_idx[h0 + k];
+    for (int k = threadIdx.x; k < nsl; k += NT) {
         lcs[k] = D.lcol[S0 + k];
         val32s[k] = D.val32[S0 + k];
     }
@@ -1137,7 +1143,7 @@ __global__ void __launch_bounds__(PCG_THREADS, 2) k_pcg32m(PcgDev D)
     int wmax = 0;
 #pragma unroll
     for (int k = 0; k < RMAX; ++k) {
-        const int sl = s_beg + warp + PCG_WARPS * k;
+        const int sl = s_beg + warp + (NT / 32) * k;
         row[k] = (sl < s_end) ? sl * 32 + lane : -1;
         lbase[k] = 0;
         wr[k] = 0;
@@ -1185,16 +1191,16 @@ __global__ void __launch_bounds__(PCG_THREADS, 2) k_pcg32m(PcgDev D)
     };
     auto stage64 = [&](const double* x) {
         __syncthreads();
-        for (int k0 = threadIdx.x; k0 < nh; k0 += 4 * PCG_THREADS) {
+        for (int k0 = threadIdx.x; k0 < nh; k0 += 4 * NT) {
             double a[4];
 #pragma unroll
             for (int u = 0; u < 4; ++u) {
-                const int k = k0 + u * PCG_THREADS;
+                const int k = k0 + u * NT;
                 a[u] = __ldcg(x + (k < nh ? hidx[k] : 0));
             }
 #pragma unroll
             for (int u = 0; u < 4; ++u)
-                if (k0 + u * PCG_THREADS < nh) vh64[k0 + u * PCG_THREADS] = a[u];
+                if (k0 + u * NT < nh) vh64[k0 + u * NT] = a[u];
         }
         __syncthreads();
     };
@@ -1226,18 +1232,18 @@ __global__ void __launch_bounds__(PCG_THREADS, 2) k_pcg32m(PcgDev D)
     // (z + beta p).A(z + beta p) follows directly
     auto refresh_ws = [&](int buf, bool zero_p, Acc8& acc) {
         __syncthreads();
-        for (int k0 = threadIdx.x; k0 < nh; k0 += 4 * PCG_THREADS) {
+        for (int k0 = threadIdx.x; k0 < nh; k0 += 4 * NT) {
             float a[4], c[4];
 #pragma unroll
             for (int u = 0; u < 4; ++u) {
-                const int k = k0 + u * PCG_THREADS;
+                const int k = k0 + u * NT;
                 const int j = k < nh ? hidx[k] : 0;
                 a[u] = __ldcg(rb[buf] + j);
                 c[u] = zero_p ? 0.0f : __ldcg(pb + j);
             }
 #pragma unroll
             for (int u = 0; u < 4; ++u) {
-                const int k = k0 + u * PCG_THREADS;
+                const int k = k0 + u * NT;
                 if (k < nh) { vz[k] = a[u] / dzh[k]; vp[k] = c[u]; }
             }
         }
@@ -1285,7 +1291,7 @@ __global__ void __launch_bounds__(PCG_THREADS, 2) k_pcg32m(PcgDev D)
     }
     true_residual(0, acc);
     Acc6 t{0.0, 0.0, 0.0, 0.0, 0.0};
-    if (!grid_allreduce3(acc, D, g, phase, t)) return;
+    if (!grid_allreduce3<NT>(acc, D, g, phase, t)) return;
     ++phase;
     const double init = sqrt(t.c);
     if (init <= 1.0e-300) { cg_finish(D, g, 0, 1, init, init, 0.0, t.mx); return; }
@@ -1296,11 +1302,11 @@ __global__ void __launch_bounds__(PCG_THREADS, 2) k_pcg32m(PcgDev D)
 
     // ---- phase 0b: z0, w0 = A z0 (p = 0, s = 0)
     __syncthreads();
-    for (int k = threadIdx.x; k < nh; k += PCG_THREADS) dzh[k] = __ldcg(dz + hidx[k]);
+    for (int k = threadIdx.x; k < nh; k += NT) dzh[k] = __ldcg(dz + hidx[k]);
     Acc8 a8{0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
     refresh_ws(0, true, a8);
     Acc8 t8{0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
-    if (!grid_allreduce5(a8, D, g, phase, t8)) return;
+    if (!grid_allreduce5<NT>(a8, D, g, phase, t8)) return;
     ++phase;
     double gam = t8.a;
     if (gam <= 1.0e-300 || !isfinite(gam)) { if (b == 0 && threadIdx.x == 0) set_status(seg_status(D, g), 3, ST_PCG, 0, R_PCG_RZ0); return; }
@@ -1317,11 +1323,11 @@ __global__ void __launch_bounds__(PCG_THREADS, 2) k_pcg32m(PcgDev D)
             const float* so = sb[po];
             const float* wo = wb[po];
             const float* ro = rb[po];
-            for (int k0 = threadIdx.x; k0 < nh; k0 += 4 * PCG_THREADS) {
+            for (int k0 = threadIdx.x; k0 < nh; k0 += 4 * NT) {
                 float a[4], c[4], e[4];
 #pragma unroll
                 for (int u = 0; u < 4; ++u) {
-                    const int k = k0 + u * PCG_THREADS;
+                    const int k = k0 + u * NT;
                     const int j = k < nh ? hidx[k] : 0;
                     a[u] = __ldcg(so + j);
                     c[u] = __ldcg(wo + j);
@@ -1329,7 +1335,7 @@ __global__ void __launch_bounds__(PCG_THREADS, 2) k_pcg32m(PcgDev D)
                 }
 #pragma unroll
                 for (int u = 0; u < 4; ++u) {
-                    const int k = k0 + u * PCG_THREADS;
+                    const int k = k0 + u * NT;
                     if (k < nh) {
                         const float sj = fmaf(b32, a[u], c[u]);
                         const float rj = fmaf(-a32, sj, e[u]);
@@ -1370,7 +1376,7 @@ __global__ void __launch_bounds__(PCG_THREADS, 2) k_pcg32m(PcgDev D)
             }
         }
         t = Acc6{0.0, 0.0, 0.0, 0.0, 0.0};
-        if (!grid_allreduce3(a6, D, g, phase, t)) return;
+        if (!grid_allreduce3<NT>(a6, D, g, phase, t)) return;
         ++phase;
         if (t.flag > 0.0) { if (b == 0 && threadIdx.x == 0) set_status(seg_status(D, g), 4, ST_PCG, it, R_PCG_RESID); return; }
         fin = sqrt(t.c);
@@ -1382,7 +1388,7 @@ __global__ void __launch_bounds__(PCG_THREADS, 2) k_pcg32m(PcgDev D)
             Acc6 u1{0.0, 0.0, 0.0, 0.0, 0.0};
             true_residual(pn, u1);
             t = Acc6{0.0, 0.0, 0.0, 0.0, 0.0};
-            if (!grid_allreduce3(u1, D, g, phase, t)) return;
+            if (!grid_allreduce3<NT>(u1, D, g, phase, t)) return;
             ++phase;
             ++outer;
             last_fix = it;
@@ -1398,7 +1404,7 @@ __global__ void __launch_bounds__(PCG_THREADS, 2) k_pcg32m(PcgDev D)
             Acc8 u2{0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
             refresh_ws(pn, restart, u2);
             t8 = Acc8{0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
-            if (!grid_allreduce5(u2, D, g, phase, t8)) return;
+            if (!grid_allreduce5<NT>(u2, D, g, phase, t8)) return;
             ++phase;
             const double gn = t8.a;
             if (gn <= 1.0e-300 || !isfinite(gn)) { if (b == 0 && threadIdx.x == 0) set_status(seg_status(D, g), 3, ST_PCG, it, R_PCG_RZ); return; }
@@ -1449,6 +1455,35 @@ cbs3d_status selftest_wait_timeout(int device, int* observed)
 }
 
 // ============================================================ PcgEngine
+namespace {
+
+// Instantiations of the single-reduction kernels by rows per thread, batch
+// mode and CTA size.
+template <bool BATCH, int NT>
+const void* fn_cgcg(int rmax)
+{
+    return rmax == 1 ? reinterpret_cast<const void*>(k_pcg64c<1, BATCH, NT>)
+         : rmax == 2 ? reinterpret_cast<const void*>(k_pcg64c<2, BATCH, NT>)
+         : rmax == 4 ? reinterpret_cast<const void*>(k_pcg64c<4, BATCH, NT>)
+                     : reinterpret_cast<const void*>(k_pcg64c<8, BATCH, NT>);
+}
+template <bool BATCH, int NT>
+const void* fn_mixed(int rmax)
+{
+    return rmax == 1 ? reinterpret_cast<const void*>(k_pcg32m<1, BATCH, NT>)
+         : rmax == 2 ? reinterpret_cast<const void*>(k_pcg32m<2, BATCH, NT>)
+         : rmax == 4 ? reinterpret_cast<const void*>(k_pcg32m<4, BATCH, NT>)
+                     : reinterpret_cast<const void*>(k_pcg32m<8, BATCH, NT>);
+}
+const void* fn_cgcg_single(int rmax, int nt) { return nt == 256 ? fn_cgcg<false, 256>(rmax) : fn_cgcg<false, 512>(rmax); }
+const void* fn_mixed_single(int rmax, int nt) { return nt == 256 ? fn_mixed<false, 256>(rmax) : fn_mixed<false, 512>(rmax); }
+
+// The batch runs 256-thread CTAs, two per SM: its instances are small and
+// many, and more, smaller CTAs spread them better.
+constexpr int BATCH_THREADS = 256;
+
+}  // namespace
+
 void PcgEngine::init(const HostModel& m, const uint8_t* nflag, const double* pfix, DevStatus* status,
                      int device, int blocks_override, bool mixed_mode, int kernel_choice)
 {
@@ -1516,18 +1551,21 @@ void PcgEngine::init(const HostModel& m, const uint8_t* nflag, const double* pfi
     if (kernel_choice == 0 || kernel_choice == 3 || kernel_choice == 4) {
         const void* hc3[4] = {reinterpret_cast<const void*>(k_pcg64h<1>), reinterpret_cast<const void*>(k_pcg64h<2>),
                               reinterpret_cast<const void*>(k_pcg64h<4>), reinterpret_cast<const void*>(k_pcg64h<8>)};
-        const void* hc4[4] = {reinterpret_cast<const void*>(k_pcg64c<1, false>), reinterpret_cast<const void*>(k_pcg64c<2, false>),
-                              reinterpret_cast<const void*>(k_pcg64c<4, false>), reinterpret_cast<const void*>(k_pcg64c<8, false>)};
         const int want = kernel_choice == 3 ? 3 : 4;
+        // CTA size of the single-reduction kernel: one 512-thread CTA per SM
+        // once every warp of such a grid has rows (fewer partials per
+        // all-reduce), two 256-thread CTAs per SM below that
+        const int nt = (want == 4 && nslices < 16 * sms) ? 256 : 512;
+        const int nwarps = nt / 32;
         for (int c = 0; c < 4 && variant == 1; ++c) {
-            const void* fn = want == 4 ? hc4[c] : hc3[c];
+            const void* fn = want == 4 ? fn_cgcg_single(rm[c], nt) : hc3[c];
             int per_sm = 0;
-            CUDA_OK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, PCG_THREADS, 0));
+            CUDA_OK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, nt, 0));
             int g = sms * (per_sm < 2 ? per_sm : 2);
             if (blocks_override > 0 && blocks_override < g) g = blocks_override;
             if (g > nslices) g = nslices > 0 ? nslices : 1;
             const int per_cta = (nslices + g - 1) / g;
-            if ((per_cta + PCG_WARPS - 1) / PCG_WARPS > rm[c]) continue;
+            if ((per_cta + nwarps - 1) / nwarps > rm[c]) continue;
             // halo of every CTA: distinct columns of its slot range, sorted
             std::vector<int> hptr(static_cast<size_t>(g) + 1, 0), hidx;
             std::vector<unsigned short> lcol(static_cast<size_t>(nslots), 0);
@@ -1555,9 +1593,10 @@ void PcgEngine::init(const HostModel& m, const uint8_t* nflag, const double* pfi
             const size_t smem = static_cast<size_t>(hmax) * (want == 4 ? 20 : 12) + static_cast<size_t>(smax) * 2 + 16;
             if (smem > 200 * 1024) continue;
             CUDA_OK(raise_smem_limit(fn, smem));
-            CUDA_OK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, PCG_THREADS, smem));
+            CUDA_OK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, nt, smem));
             if (per_sm * sms < g) continue;
             variant = want;
+            nthreads = nt;
             rmax = rm[c];
             nblocks = g;
             halo_smem = smem;
@@ -1570,13 +1609,13 @@ void PcgEngine::init(const HostModel& m, const uint8_t* nflag, const double* pfi
             dev_halo_max = hmax;
             dev_slot_max = static_cast<int>(smax);
             if (mixed && want == 4) {
-                const void* mc[4] = {reinterpret_cast<const void*>(k_pcg32m<1, false>), reinterpret_cast<const void*>(k_pcg32m<2, false>),
-                                     reinterpret_cast<const void*>(k_pcg32m<4, false>), reinterpret_cast<const void*>(k_pcg32m<8, false>)};
+                const void* mc[4] = {fn_mixed_single(1, nt), fn_mixed_single(2, nt), fn_mixed_single(4, nt),
+                                     fn_mixed_single(8, nt)};
                 const size_t ms = static_cast<size_t>(hmax) * 16 + static_cast<size_t>(smax) * 6 + 16;
                 int per = 0;
                 if (ms <= 220 * 1024 &&
                     raise_smem_limit(mc[c], ms) == cudaSuccess &&
-                    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, mc[c], PCG_THREADS, ms) == cudaSuccess &&
+                    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, mc[c], nt, ms) == cudaSuccess &&
                     per * sms >= g) {
                     mixed_ok = true;
                     mixed_smem = ms;
@@ -1677,20 +1716,14 @@ cbs3d_status PcgEngine::solve(double* pres, double* rhs1, double* pdiag, int pre
         else fn = reinterpret_cast<const void*>(k_pcg64h<8>);
         smem = halo_smem;
     } else if (variant == 4 && mixed_ok) {
-        if (rmax == 1) fn = reinterpret_cast<const void*>(k_pcg32m<1, false>);
-        else if (rmax == 2) fn = reinterpret_cast<const void*>(k_pcg32m<2, false>);
-        else if (rmax == 4) fn = reinterpret_cast<const void*>(k_pcg32m<4, false>);
-        else fn = reinterpret_cast<const void*>(k_pcg32m<8, false>);
+        fn = fn_mixed_single(rmax, nthreads);
         smem = mixed_smem;
     } else if (variant == 4) {
-        if (rmax == 1) fn = reinterpret_cast<const void*>(k_pcg64c<1, false>);
-        else if (rmax == 2) fn = reinterpret_cast<const void*>(k_pcg64c<2, false>);
-        else if (rmax == 4) fn = reinterpret_cast<const void*>(k_pcg64c<4, false>);
-        else fn = reinterpret_cast<const void*>(k_pcg64c<8, false>);
+        fn = fn_cgcg_single(rmax, nthreads);
         smem = halo_smem;
     }
     if (ev0) CUDA_OK(cudaEventRecord(ev0, st));
-    CUDA_OK(cudaLaunchCooperativeKernel(fn, dim3(nblocks), dim3(PCG_THREADS), args, smem, st));
+    CUDA_OK(cudaLaunchCooperativeKernel(fn, dim3(nblocks), dim3(nthreads), args, smem, st));
     if (ev1) CUDA_OK(cudaEventRecord(ev1, st));
     k_perm_out<<<(NP + 255) / 256, 256, 0, st>>>(D, d_xp, pres);
     if (sync) CUDA_OK(cudaStreamSynchronize(st));
@@ -1755,7 +1788,7 @@ void PcgBatch::init(const std::vector<PcgBatchMember>& members, int dev_id, bool
     mixed = mixed_mode;
     const size_t K = mem.size();
     CUDA_OK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
-    gmax = 2 * sms;   // two 256-thread CTAs per SM at 128 registers
+    gmax = 2 * sms;   // two BATCH_THREADS CTAs per SM
     slice0.assign(K, 0); nsl.assign(K, 0); N_k.assign(K, 0);
     slot0.assign(K, 0); nslot.assign(K, 0);
     nslices = 0; nslots = 0;
@@ -1851,7 +1884,7 @@ bool PcgBatch::plan(const PcgBatchPlan& p, std::string* why)
         return false;
     }
     const int K = static_cast<int>(mem.size());
-    const int cap = PCG_WARPS * p.rmax;   // slices one CTA holds in registers
+    const int cap = (BATCH_THREADS / 32) * p.rmax;   // slices one CTA holds in registers
     std::vector<int> minc(static_cast<size_t>(K));
     for (int k = 0; k < K; ++k) {
         minc[static_cast<size_t>(k)] = std::max(1, (nsl[static_cast<size_t>(k)] + cap - 1) / cap);
@@ -1873,10 +1906,10 @@ bool PcgBatch::plan(const PcgBatchPlan& p, std::string* why)
         packs[w].push_back(k);
         used[w] += minc[static_cast<size_t>(k)];
     }
-    const void* c64[4] = {reinterpret_cast<const void*>(k_pcg64c<1, true>), reinterpret_cast<const void*>(k_pcg64c<2, true>),
-                          reinterpret_cast<const void*>(k_pcg64c<4, true>), reinterpret_cast<const void*>(k_pcg64c<8, true>)};
-    const void* c32[4] = {reinterpret_cast<const void*>(k_pcg32m<1, true>), reinterpret_cast<const void*>(k_pcg32m<2, true>),
-                          reinterpret_cast<const void*>(k_pcg32m<4, true>), reinterpret_cast<const void*>(k_pcg32m<8, true>)};
+    const void* c64[4] = {fn_cgcg<true, BATCH_THREADS>(1), fn_cgcg<true, BATCH_THREADS>(2), fn_cgcg<true, BATCH_THREADS>(4),
+                          fn_cgcg<true, BATCH_THREADS>(8)};
+    const void* c32[4] = {fn_mixed<true, BATCH_THREADS>(1), fn_mixed<true, BATCH_THREADS>(2), fn_mixed<true, BATCH_THREADS>(4),
+                          fn_mixed<true, BATCH_THREADS>(8)};
     const int ci = p.rmax == 1 ? 0 : p.rmax == 2 ? 1 : p.rmax == 4 ? 2 : 3;
 
     struct HostWave {
@@ -1967,7 +2000,7 @@ bool PcgBatch::plan(const PcgBatchPlan& p, std::string* why)
                 return false;
             }
             int per = 0;
-            if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, fn, PCG_THREADS, smem) != cudaSuccess) {
+            if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, fn, BATCH_THREADS, smem) != cudaSuccess) {
                 cudaGetLastError();
                 return false;
             }
@@ -2050,7 +2083,7 @@ void PcgBatch::solve(cudaStream_t st)
     CUDA_OK(cudaMemsetAsync(d_out, 0, mem.size() * sizeof(CgOut), st));
     for (Wave& W : waves) {
         void* args[] = {&W.dev};
-        CUDA_OK(cudaLaunchCooperativeKernel(W.fn, dim3(static_cast<unsigned>(W.G)), dim3(PCG_THREADS), args, W.smem, st));
+        CUDA_OK(cudaLaunchCooperativeKernel(W.fn, dim3(static_cast<unsigned>(W.G)), dim3(BATCH_THREADS), args, W.smem, st));
     }
 }
 

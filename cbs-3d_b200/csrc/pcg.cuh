@@ -91,6 +91,7 @@ public:
 
     bool mixed = false;
     int rmax = 0;            // rows per thread of the register-resident kernels (0: global kernel)
+    int nthreads = 512;      // CTA size of the persistent kernel
     int variant = 1;         // 1 global vectors, 2 register rows, 3 + shared-memory halo, 4 + one sync per iteration
     size_t halo_smem = 0;    // dynamic shared memory of the halo kernel
     size_t mixed_smem = 0;   // dynamic shared memory of the mixed-precision kernel
