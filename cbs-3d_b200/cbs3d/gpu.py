@@ -231,7 +231,7 @@ def case_digest(case_name: str, use_cache: bool = False):
     return d.value, bool(hit.value)
 
 
-def make_options(precision: int = FP64, device: int = 0, inner_tol: float = 1e-5, use_graph: bool = True,
+def make_options(precision: int = FP64, device: int = 0, inner_tol: float = 0.05, use_graph: bool = True,
                  pcg_blocks: int = 0, time_pcg: bool = False, pcg_kernel: int = 0) -> Options:
     o = Options()
     lib().cbs3d_default_options(ctypes.byref(o))
@@ -273,7 +273,7 @@ class Context:
     """One case resident on the GPU."""
 
     def __init__(self, case=None, case_name: str | None = None, precision: int = FP64, device: int = 0,
-                 inner_tol: float = 1e-5, use_graph: bool = True, pcg_blocks: int = 0, time_pcg: bool = False,
+                 inner_tol: float = 0.05, use_graph: bool = True, pcg_blocks: int = 0, time_pcg: bool = False,
                  pcg_kernel: int = 0, case_cache: bool = False):
         L = lib()
         self.h = ctypes.c_void_p()
@@ -425,7 +425,7 @@ class PressureSolver:
     """Drop-in for ConjugateGradient::solvePressure on the GPU."""
 
     def __init__(self, intma, mat_elem, bc_list, bc_values, precision: int = FP64, device: int = 0,
-                 inner_tol: float = 1e-5):
+                 inner_tol: float = 0.05):
         L = lib()
         self.h = ctypes.c_void_p()
         intma = np.ascontiguousarray(intma, dtype=np.int32).reshape(-1)
@@ -505,7 +505,7 @@ class Batch:
     per wave of instances."""
 
     def __init__(self, cases, precision: int = FP64, device: int = 0, autotune: bool = True,
-                 rows_per_thread: int = 4, spread: bool = True, use_graph: bool = True, inner_tol: float = 1e-5):
+                 rows_per_thread: int = 4, spread: bool = True, use_graph: bool = True, inner_tol: float = 0.05):
         L = lib()
         self.h = ctypes.c_void_p()
         self.n = len(cases)

@@ -650,7 +650,7 @@ public:
     void solve(double* x, double* b)
     {
         if (!pcg_ready) {
-            pcg.inner_tol = 1.0e-5;
+            pcg.inner_tol = 0.05;
             pcg.init(c.m, c.S.nflag, zpfix, c.S.status, c.opt.device, 0, false, 0);
             pcg_ready = true;
         }

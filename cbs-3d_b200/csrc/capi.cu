@@ -196,7 +196,7 @@ void cbs3d_ctx::setup(bool own_pcg)
     CUDA_OK(cudaStreamSynchronize(st));
     check_status();
     if (!own_pcg) return;
-    pcg.inner_tol = opt.inner_tol > 0.0 ? opt.inner_tol : 1.0e-5;
+    pcg.inner_tol = opt.inner_tol > 0.0 ? opt.inner_tol : 0.05;
     pcg.init(m, S.nflag, S.pfix, S.status, opt.device, opt.pcg_blocks, opt.precision == CBS3D_MIXED, opt.pcg_kernel);
 }
 
@@ -346,7 +346,7 @@ void cbs3d_default_options(cbs3d_options* o)
     if (!o) return;
     std::memset(o, 0, sizeof *o);
     o->precision = CBS3D_FP64;
-    o->inner_tol = 1.0e-5;
+    o->inner_tol = 0.05;
     o->use_graph = 1;
 }
 
@@ -853,7 +853,7 @@ cbs3d_status cbs3d_pcg_create(int nelem, int npoin, const int* intma, const int*
         p->d_pres = p->buf.alloc<double>(N);
         p->d_rhs1 = p->buf.alloc<double>(N);
         p->d_pdiag = p->buf.alloc<double>(N);
-        p->eng.inner_tol = p->opt.inner_tol > 0.0 ? p->opt.inner_tol : 1.0e-5;
+        p->eng.inner_tol = p->opt.inner_tol > 0.0 ? p->opt.inner_tol : 0.05;
         p->eng.init(m, p->d_nflag, p->d_pfix, p->d_status, p->opt.device, p->opt.pcg_blocks,
                     p->opt.precision == CBS3D_MIXED, p->opt.pcg_kernel);
         *out = p.release();
@@ -1116,7 +1116,7 @@ cbs3d_status cbs3d_batch_create(int n, const cbs3d_mesh* meshes, const cbs3d_par
             b->done_pre.push_back(e1);
             b->done_post.push_back(e2);
         }
-        const double itol = b->opt.base.inner_tol > 0.0 ? b->opt.base.inner_tol : 1.0e-5;
+        const double itol = b->opt.base.inner_tol > 0.0 ? b->opt.base.inner_tol : 0.05;
         b->pcg.init(mem, b->opt.base.device, b->opt.base.precision == CBS3D_MIXED, itol);
         for (int i = 0; i < n; ++i) b->inst[static_cast<size_t>(i)]->batch_out = b->pcg.out(i);
         PcgBatchPlan p;

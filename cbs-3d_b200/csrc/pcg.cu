@@ -1091,7 +1091,7 @@ __global__ void __launch_bounds__(NT, NT >= 512 ? 1 : 2) k_pcg64c(PcgDev D)
 // column indices resident in shared memory for the whole solve -- with the
 // reductions, alpha/beta and the pressure in FP64, and FP64 defect
 // correction by residual replacement: whenever the recursive residual has
-// fallen by RU_FACTOR since the last correction, and whenever it meets the
+// fallen by the inner tolerance since the last correction, and whenever it meets the
 // stopping test, the true residual r = b - A x is recomputed from the FP64
 // coefficients and FP64 pressure, and w = A z, s = A p are recomputed, so the
 // FP32 recurrences restart from exact data without discarding the search
@@ -1100,7 +1100,6 @@ __global__ void __launch_bounds__(NT, NT >= 512 ? 1 : 2) k_pcg64c(PcgDev D)
 // progress since the previous one also drops the direction.  The solve
 // stops only when the FP64 true residual meets the reference's stopping
 // test.
-constexpr double RU_FACTOR = 0.05;
 constexpr int RU_STALL = 256;   // iterations without a correction before one is forced
 
 template <int RMAX, bool BATCH, int NT>
@@ -1383,7 +1382,7 @@ __global__ void __launch_bounds__(NT, NT >= 512 ? 1 : 2) k_pcg32m(PcgDev D)
         mx = t.mx;
         rel = fin / init;
         const bool candidate = cg_converged(g.conv_test, rel, mx, g.rel_tol, g.abs_tol);
-        if (candidate || t.c <= RU_FACTOR * RU_FACTOR * rr_last || it - last_fix >= RU_STALL) {
+        if (candidate || t.c <= D.inner_tol * D.inner_tol * rr_last || it - last_fix >= RU_STALL) {
             // residual replacement from the FP64 coefficients and pressure
             Acc6 u1{0.0, 0.0, 0.0, 0.0, 0.0};
             true_residual(pn, u1);

@@ -103,7 +103,7 @@ public:
     double *d_xp = nullptr, *d_bp = nullptr, *d_dp = nullptr;   // pressure, rhs, diagonal by position
     uint8_t* d_fp = nullptr;
     int dev_halo_max = 0;
-    double inner_tol = 1.0e-5;
+    double inner_tol = 0.05;      // mixed: residual-replacement factor
     int N = 0, NP = 0, E = 0, nslices = 0, nblocks = 0;
     long long nslots = 0, ncontrib = 0;
     long long *d_slice_off = nullptr, *d_cptr = nullptr;

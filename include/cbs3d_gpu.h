@@ -90,7 +90,8 @@ typedef struct cbs3d_mesh {
 typedef struct cbs3d_options {
     int precision;           /* cbs3d_precision */
     int device;              /* CUDA device ordinal */
-    double inner_tol;        /* MIXED: relative FP32 inner tolerance (default 1e-5) */
+    double inner_tol;        /* MIXED: the FP32 recurrences are replaced by the FP64 true residual
+                                whenever the recursive residual has fallen by this factor (default 0.05) */
     int use_graph;           /* capture the per-step launch sequence in a CUDA graph */
     int pcg_blocks;          /* persistent PCG grid size; 0 = one wave of resident CTAs */
     int verbose;
