@@ -251,7 +251,7 @@ def roofline(st, warm, nelem_fluid, npoin, mixed, n):
     its = st.cg_iterations_total - warm.cg_iterations_total   # totals are cumulative
     alg = algorithmic_bytes(nelem_fluid, npoin, mixed)
     achieved = its * alg / st.pcg_seconds / 1e9 if st.pcg_seconds > 0 else None
-    names = {1: "k_pcg64", 2: "k_pcg64r", 3: "k_pcg64h", 4: "k_pcg64c", 5: "k_pcg32m"}
+    names = {1: "k_pcg64", 2: "k_pcg64r", 3: "k_pcg64h", 4: "k_pcg64c", 5: "k_pcg32m", 6: "k_pcg64d"}
     kname = names.get(st.pcg_kernel, "?")
     return {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
             "frac": achieved / peak if achieved else None, "traffic": ncu_traffic(kname, n),

@@ -79,7 +79,8 @@ class Mesh(ctypes.Structure):
 
 class Options(ctypes.Structure):
     _fields_ = [("precision", _i), ("device", _i), ("inner_tol", _d), ("use_graph", _i),
-                ("pcg_blocks", _i), ("verbose", _i), ("time_pcg", _i), ("pcg_kernel", _i), ("case_cache", _i)]
+                ("pcg_blocks", _i), ("verbose", _i), ("time_pcg", _i), ("pcg_kernel", _i), ("case_cache", _i),
+                ("pcg_two_level", _i)]
 
 
 class CGResult(ctypes.Structure):
@@ -274,13 +275,14 @@ class Context:
 
     def __init__(self, case=None, case_name: str | None = None, precision: int = FP64, device: int = 0,
                  inner_tol: float = 0.05, use_graph: bool = True, pcg_blocks: int = 0, time_pcg: bool = False,
-                 pcg_kernel: int = 0, case_cache: bool = False):
+                 pcg_kernel: int = 0, case_cache: bool = False, two_level: bool = False):
         L = lib()
         self.h = ctypes.c_void_p()
         self.device = device
         err = ctypes.create_string_buffer(1024)
         opt = make_options(precision, device, inner_tol, use_graph, pcg_blocks, time_pcg, pcg_kernel)
         opt.case_cache = 1 if case_cache else 0
+        opt.pcg_two_level = 1 if two_level else 0
         if case_name is not None:
             rc = L.cbs3d_create_from_case(case_name.encode(), ctypes.byref(opt), ctypes.byref(self.h), err, 1024)
         else:

@@ -197,7 +197,8 @@ void cbs3d_ctx::setup(bool own_pcg)
     check_status();
     if (!own_pcg) return;
     pcg.inner_tol = opt.inner_tol > 0.0 ? opt.inner_tol : 0.05;
-    pcg.init(m, S.nflag, S.pfix, S.status, opt.device, opt.pcg_blocks, opt.precision == CBS3D_MIXED, opt.pcg_kernel);
+    pcg.init(m, S.nflag, S.pfix, S.status, opt.device, opt.pcg_blocks, opt.precision == CBS3D_MIXED, opt.pcg_kernel,
+             opt.pcg_two_level > 0);
 }
 
 void cbs3d_ctx::check_status()
@@ -485,7 +486,7 @@ static DevStatus collect_call(cbs3d_ctx* c, int done, int start, long long launc
     stats->kernel_launches = c->launches - launches0;
     if (!c->batch_out) {
         stats->pcg_bytes_per_iter = static_cast<double>(c->pcg.bytes_per_iter());
-        stats->pcg_kernel = c->pcg.variant == 4 && c->pcg.mixed_ok ? 5 : c->pcg.variant;
+        stats->pcg_kernel = c->pcg.coarse ? 6 : c->pcg.variant == 4 && c->pcg.mixed_ok ? 5 : c->pcg.variant;
     }
     for (int k = 0; k + 1 < c->pcg_ev_used; k += 2) {
         float pm = 0.0f;

@@ -842,6 +842,95 @@ __device__ __forceinline__ bool grid_allreduce5(Acc8 v, const PcgDev& D, const S
     return ok;
 }
 
+// Grid all-reduce of (sum a, sum b, sum c, max mx, max flag) that also
+// gathers one per-CTA sum: every CTA's block sum of `x` lands in cvec[CTA]
+// of every CTA (the aggregated vectors of the two-level preconditioner).
+template <int NT>
+__device__ __forceinline__ bool grid_allreduce3g(Acc6 v, double x, const PcgDev& D, const SegView& g, int phase,
+                                                 Acc6& out, double* cvec)
+{
+    constexpr int NW = NT / 32;
+    __shared__ double sm[NW][6];
+    __shared__ int s_ok;
+    const int G = g.G;
+    DevStatus* status = seg_status(D, g);
+    double vv[6] = {v.a, v.b, v.c, v.mx, v.flag, x};
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1)
+#pragma unroll
+        for (int q = 0; q < 6; ++q) {
+            const double y = __shfl_down_sync(0xffffffffu, vv[q], o);
+            vv[q] = (q < 3 || q == 5) ? vv[q] + y : fmax(vv[q], y);
+        }
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    if (lane == 0)
+#pragma unroll
+        for (int q = 0; q < 6; ++q) sm[w][q] = vv[q];
+    __syncthreads();
+    unsigned long long* cnt = reinterpret_cast<unsigned long long*>(seg_bar(D, g));
+    double* part = seg_part(D, g) + (size_t)(phase & 1) * G * 8;
+    if (threadIdx.x == 0) {
+        double t[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+        for (int k = 0; k < NW; ++k)
+#pragma unroll
+            for (int q = 0; q < 6; ++q) t[q] = (q < 3 || q == 5) ? t[q] + sm[k][q] : fmax(t[q], sm[k][q]);
+        double* p = part + (size_t)g.b * 8;
+#pragma unroll
+        for (int q = 0; q < 5; ++q) __stcg(p + q, t[q]);
+        __stcg(p + 7, t[5]);
+        const unsigned long long target = (unsigned long long)(phase + 1) * (unsigned long long)G;
+        unsigned long long arrived;
+        asm volatile("atom.add.acq_rel.gpu.global.u64 %0, [%1], 1;" : "=l"(arrived) : "l"(cnt) : "memory");
+        int ok = 1;
+        if (arrived + 1 < target) {
+            const long long t0 = clock64();
+            for (;;) {
+                unsigned long long c;
+                asm volatile("ld.acquire.gpu.global.u64 %0, [%1];" : "=l"(c) : "l"(cnt) : "memory");
+                if (c >= target) break;
+                if (ld_relaxed_int(&status->code) != 0) { ok = 0; break; }
+                if (clock64() - t0 > (1LL << 31)) {
+                    set_status(status, 5 /*CBS3D_TIMEOUT*/, ST_PCG, 0, R_PCG_BARRIER);
+                    ok = 0;
+                    break;
+                }
+            }
+        }
+        if (ok && ld_relaxed_int(&status->code) != 0) ok = 0;
+        s_ok = ok;
+    }
+    __syncthreads();
+    const bool ok = s_ok != 0;
+    double t[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
+    if (ok) {
+        for (int k = threadIdx.x; k < G; k += NT) {
+            const double* p = part + (size_t)k * 8;
+#pragma unroll
+            for (int q = 0; q < 5; ++q) t[q] = q < 3 ? t[q] + __ldcg(p + q) : fmax(t[q], __ldcg(p + q));
+            cvec[k] = __ldcg(p + 7);
+        }
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1)
+#pragma unroll
+        for (int q = 0; q < 5; ++q) {
+            const double y = __shfl_down_sync(0xffffffffu, t[q], o);
+            t[q] = q < 3 ? t[q] + y : fmax(t[q], y);
+        }
+    __syncthreads();
+    if (lane == 0)
+#pragma unroll
+        for (int q = 0; q < 5; ++q) sm[w][q] = t[q];
+    __syncthreads();
+    double o5[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
+    for (int k = 0; k < NW; ++k)
+#pragma unroll
+        for (int q = 0; q < 5; ++q) o5[q] = q < 3 ? o5[q] + sm[k][q] : fmax(o5[q], sm[k][q]);
+    out = Acc6{o5[0], o5[1], o5[2], o5[3], o5[4]};
+    __syncthreads();
+    return ok;
+}
+
 template <int RMAX, bool BATCH, int NT>
 __global__ void __launch_bounds__(NT, NT >= 512 ? 1 : 2) k_pcg64c(PcgDev D)
 {
@@ -1069,6 +1158,301 @@ __global__ void __launch_bounds__(NT, NT >= 512 ? 1 : 2) k_pcg64c(PcgDev D)
         t = Acc6{0.0, 0.0, 0.0, 0.0, 0.0};
         if (!grid_allreduce3<NT>(a6, D, g, phase, t)) return;
         ++phase;
+        fin = sqrt(t.c);
+        mx = t.mx;
+        rel = fin / init;
+        if (cg_converged(g.conv_test, rel, mx, g.rel_tol, g.abs_tol)) { conv = 1; break; }
+        if (t.flag > 0.0) { if (b == 0 && threadIdx.x == 0) set_status(seg_status(D, g), 4, ST_PCG, it, R_PCG_RESID); return; }
+        const double gn = t.a;
+        if (gn <= 1.0e-300 || !isfinite(gn)) { if (b == 0 && threadIdx.x == 0) set_status(seg_status(D, g), 3, ST_PCG, it, R_PCG_RZ); return; }
+        beta = gn / gam;
+        den = t.b - beta * gn / alpha;
+        gam = gn;
+    }
+    if (it > g.max_iter) it = g.max_iter;
+    cg_finish(D, g, it, conv, init, fin, rel, mx);
+    if (!conv && b == 0 && threadIdx.x == 0) set_status(seg_status(D, g), 2, ST_PCG, it, R_PCG_MAXIT);
+}
+
+template <int RMAX>
+__global__ void __launch_bounds__(512, 1) k_pcg64d(PcgDev D, CoarseDev C)
+{
+    constexpr bool BATCH = false;
+    constexpr int NT = 512;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const SegView g = seg_view<BATCH>(D);
+    const int G = g.G, b = g.b;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int s_beg = g.s0 + (int)((long long)b * (g.s1 - g.s0) / G);
+    const int s_end = g.s0 + (int)((long long)(b + 1) * (g.s1 - g.s0) / G);
+    const long long S0 = D.slice_off[s_beg];
+    const int nsl = (int)(D.slice_off[s_end] - S0);
+    const int h0 = D.halo_ptr[blockIdx.x];
+    const int nh = D.halo_ptr[blockIdx.x + 1] - h0;
+    double* vh = reinterpret_cast<double*>(smem_raw);
+    double* dzh = vh + D.halo_max;
+    int* hidx = reinterpret_cast<int*>(dzh + D.halo_max);
+    unsigned short* lcs = reinterpret_cast<unsigned short*>(hidx + D.halo_max);
+    for (int k = threadIdx.x; k < nh; k += NT) hidx[k] = D.halo_idx[h0 + k];
+    for (int k = threadIdx.x; k < nsl; k += NT) lcs[k] = D.lcol[S0 + k];
+    // coarse space: this CTA's rows of the coarse inverse (its own and its
+    // halo's owners), the coarse vectors P^T r, P^T s, P^T w, the coarse
+    // correction of each neighbour and the owner of every halo entry
+    const int GC = C.G;
+    const int nb0 = C.nbr_ptr[blockIdx.x];
+    const int nn = C.nbr_ptr[blockIdx.x + 1] - nb0;
+    double* ainv = reinterpret_cast<double*>(
+        (reinterpret_cast<uintptr_t>(lcs + D.slot_max) + 15) & ~static_cast<uintptr_t>(15));
+    double* cr = ainv + (size_t)C.nbr_max * GC;
+    double* cs = cr + GC;
+    double* cw = cs + GC;
+    double* ec = cw + GC;
+    unsigned char* hown = reinterpret_cast<unsigned char*>(ec + C.nbr_max);
+    __shared__ int s_own;
+    __shared__ double s_ecp;   // this CTA's coarse correction of the previous iteration's z
+    if (threadIdx.x == 0)
+        for (int j = 0; j < nn; ++j)
+            if (C.nbr_ids[nb0 + j] == (int)blockIdx.x) s_own = j;
+    for (int t = threadIdx.x; t < nn * GC; t += NT)
+        ainv[t] = C.ainv[(size_t)C.nbr_ids[nb0 + t / GC] * GC + t % GC];
+    for (int k = threadIdx.x; k < nh; k += NT) hown[k] = C.hown[h0 + k];
+    for (int t = threadIdx.x; t < GC; t += NT) cs[t] = 0.0;
+    // ec[j] = (A_c^-1 P^T r)[neighbour j]: one warp per neighbour, fixed order
+    auto coarse_correction = [&]() {
+        __syncthreads();
+        for (int j = warp; j < nn; j += NT / 32) {
+            double acc = 0.0;
+            for (int t = lane; t < GC; t += 32) acc = fma(ainv[(size_t)j * GC + t], cr[t], acc);
+            for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
+            if (lane == 0) ec[j] = acc;
+        }
+        __syncthreads();
+    };
+    int phase = 0;
+    const int N = D.N;
+    // parity buffers: r in r/pA, w in q/pB, s in z/dz(+N)... laid out by the engine
+    double* rb[2] = {D.r, D.r + N};
+    double* wb[2] = {D.q, D.q + N};
+    double* sb[2] = {D.pA, D.pB};
+    double* dz = D.z;   // free ? diagonal : +inf  (z = r / dz)
+
+    // rows of this thread: slice s_beg + warp + NW*k, lane; their slot base
+    // and width are re-read where needed (registers go to the coarse state)
+    double r[RMAX], p[RMAX], s[RMAX], w[RMAX], dd[RMAX];
+    bool fr[RMAX];
+    int wmax = 0;
+    auto slice_of = [&](int k) { return s_beg + warp + (NT / 32) * k; };
+    auto row_of = [&](int k) { const int sl = slice_of(k); return sl < s_end ? sl * 32 + lane : -1; };
+    auto width_of = [&](int k) { const int sl = slice_of(k); return sl < s_end ? D.slice_w[sl] : 0; };
+    auto base_of = [&](int k) { const int sl = slice_of(k); return sl < s_end ? (int)(D.slice_off[sl] - S0) + lane : 0; };
+#pragma unroll
+    for (int k = 0; k < RMAX; ++k) {
+        const int wk = width_of(k);
+        wmax = wk > wmax ? wk : wmax;
+        r[k] = p[k] = s[k] = w[k] = 0.0;
+        dd[k] = __longlong_as_double(0x7ff0000000000000LL);
+        fr[k] = false;
+    }
+    constexpr int CH = (RMAX >= 8) ? 2 : (RMAX >= 4) ? 4 : 8;
+    auto offdiag_all = [&](double* off) {
+        int lbase[RMAX], wr[RMAX];
+#pragma unroll
+        for (int k = 0; k < RMAX; ++k) { off[k] = 0.0; lbase[k] = base_of(k); wr[k] = width_of(k); }
+        for (int k0 = 0; k0 < wmax; k0 += CH) {
+            double v[RMAX][CH];
+#pragma unroll
+            for (int k = 0; k < RMAX; ++k)
+#pragma unroll
+                for (int u = 0; u < CH; ++u)
+                    v[k][u] = (k0 + u < wr[k]) ? __ldcg(D.val + S0 + lbase[k] + 32 * (k0 + u)) : 0.0;
+#pragma unroll
+            for (int k = 0; k < RMAX; ++k)
+#pragma unroll
+                for (int u = 0; u < CH; ++u) {
+                    const double g = (k0 + u < wr[k]) ? vh[lcs[lbase[k] + 32 * (k0 + u)]] : 0.0;
+                    off[k] = fma(v[k][u], g, off[k]);
+                }
+        }
+    };
+
+    // ---- phase 0a: r0 = b - A x0 (constraints as the reference), dz
+    double off[RMAX];
+    __syncthreads();
+    for (int k0 = threadIdx.x; k0 < nh; k0 += 4 * NT) {
+        double a[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            const int k = k0 + u * NT;
+            a[u] = __ldcg(D.pres + (k < nh ? hidx[k] : 0));
+        }
+#pragma unroll
+        for (int u = 0; u < 4; ++u)
+            if (k0 + u * NT < nh) vh[k0 + u * NT] = a[u];
+    }
+    __syncthreads();
+    offdiag_all(off);
+    Acc6 acc{0.0, 0.0, 0.0, 0.0, 0.0};
+#pragma unroll
+    for (int k = 0; k < RMAX; ++k) {
+        const int i = row_of(k);
+        if (i < 0) continue;
+        const uint8_t f = D.nflag[i];
+        const bool active = f & 1;
+        fr[k] = (f & 1) && !(f & 4);
+        const double pd = D.pdiag[i];
+        const double y = fma(pd, D.pres[i], off[k]);
+        double ri = active ? D.rhs1[i] - y : 0.0;
+        if (!fr[k]) ri = 0.0;
+        if (fr[k]) {
+            if (g.precond) {
+                if (!(isfinite(pd) && pd > 1.0e-30)) acc.flag = fmax(acc.flag, 1.0);
+                dd[k] = pd;
+            } else {
+                dd[k] = 1.0;
+            }
+            if (!isfinite(ri)) acc.flag = fmax(acc.flag, 2.0);
+            acc.c = fma(ri, ri, acc.c);
+            acc.mx = fmax(acc.mx, fabs(ri));
+        }
+        r[k] = ri;
+        rb[0][i] = ri;
+        dz[i] = dd[k];
+        sb[0][i] = 0.0;
+    }
+    double xs = 0.0;
+#pragma unroll
+    for (int k = 0; k < RMAX; ++k) xs += r[k];
+    Acc6 t{0.0, 0.0, 0.0, 0.0, 0.0};
+    if (!grid_allreduce3g<NT>(acc, xs, D, g, phase, t, cr)) return;
+    ++phase;
+    const double init = sqrt(t.c);
+    if (init <= 1.0e-300) { cg_finish(D, g, 0, 1, init, init, 0.0, t.mx); return; }
+    if (cg_converged(g.conv_test, 1.0, t.mx, g.rel_tol, g.abs_tol)) { cg_finish(D, g, 0, 1, init, init, 1.0, t.mx); return; }
+    if (t.flag >= 2.0) { if (b == 0 && threadIdx.x == 0) set_status(seg_status(D, g), 4, ST_PCG, 0, R_PCG_RESID); return; }
+    if (t.flag >= 1.0) { if (b == 0 && threadIdx.x == 0) set_status(seg_status(D, g), 1, ST_PCG, 0, R_PCG_DIAG); return; }
+
+    // ---- phase 0b: z0 = M^-1 r0, w0 = A z0, gamma0 = (r0,z0), delta0 = (z0,w0)
+    coarse_correction();
+    for (int k0 = threadIdx.x; k0 < nh; k0 += 4 * NT) {
+        double a[4], c[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            const int k = k0 + u * NT;
+            const int j = k < nh ? hidx[k] : 0;
+            a[u] = __ldcg(dz + j);
+            c[u] = __ldcg(rb[0] + j);
+        }
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            const int k = k0 + u * NT;
+            if (k < nh) { dzh[k] = a[u]; vh[k] = isfinite(a[u]) ? c[u] / a[u] + ec[hown[k]] : 0.0; }
+        }
+    }
+    __syncthreads();
+    offdiag_all(off);
+    acc = Acc6{0.0, 0.0, 0.0, 0.0, 0.0};
+#pragma unroll
+    for (int k = 0; k < RMAX; ++k) {
+        const int i = row_of(k);
+        if (i < 0) continue;
+        const double zi = fr[k] ? r[k] / dd[k] + ec[s_own] : 0.0;
+        w[k] = fr[k] ? fma(D.pdiag[i], zi, off[k]) : 0.0;
+        wb[0][i] = w[k];
+        if (fr[k]) {
+            acc.a = fma(r[k], zi, acc.a);
+            acc.b = fma(zi, w[k], acc.b);
+        }
+    }
+    xs = 0.0;
+#pragma unroll
+    for (int k = 0; k < RMAX; ++k) xs += w[k];
+    t = Acc6{0.0, 0.0, 0.0, 0.0, 0.0};
+    if (!grid_allreduce3g<NT>(acc, xs, D, g, phase, t, cw)) return;
+    ++phase;
+    if (threadIdx.x == 0) s_ecp = ec[s_own];
+    double gam = t.a;
+    if (gam <= 1.0e-300 || !isfinite(gam)) { if (b == 0 && threadIdx.x == 0) set_status(seg_status(D, g), 3, ST_PCG, 0, R_PCG_RZ0); return; }
+    double den = t.b;
+    double beta = 0.0, fin = init, rel = 1.0, mx = 0.0, alpha = 0.0;
+    int it = 0, conv = 0;
+    for (it = 1; it <= g.max_iter; ++it) {
+        if (fabs(den) <= 1.0e-300 || !isfinite(den)) { if (b == 0 && threadIdx.x == 0) set_status(seg_status(D, g), 3, ST_PCG, it, R_PCG_PAP); return; }
+        alpha = gam / den;
+        const int po = (it - 1) & 1, pn = it & 1;
+        // P^T s = P^T w_o + beta P^T s_o, P^T r = P^T r_o - alpha P^T s (the
+        // recurrences of s and r, aggregated), then the new coarse correction
+        for (int c = threadIdx.x; c < GC; c += NT) {
+            cs[c] = fma(beta, cs[c], cw[c]);
+            cr[c] = fma(-alpha, cs[c], cr[c]);
+        }
+        coarse_correction();
+        // stage z_it of the halo: s = w_o + beta*s_o, r = r_o - alpha*s, z = r / dz
+        // (SU halo nodes per thread per round, all their loads issued first)
+        __syncthreads();
+        {
+            constexpr int SU = 4;
+            const double* so = sb[po];
+            const double* wo = wb[po];
+            const double* ro = rb[po];
+            for (int k0 = threadIdx.x; k0 < nh; k0 += SU * NT) {
+                double a[SU], c[SU], e[SU];
+#pragma unroll
+                for (int u = 0; u < SU; ++u) {
+                    const int k = k0 + u * NT;
+                    const int j = k < nh ? hidx[k] : 0;
+                    a[u] = __ldcg(so + j);
+                    c[u] = __ldcg(wo + j);
+                    e[u] = __ldcg(ro + j);
+                }
+#pragma unroll
+                for (int u = 0; u < SU; ++u) {
+                    const int k = k0 + u * NT;
+                    if (k < nh) {
+                        const double sj = fma(beta, a[u], c[u]);
+                        const double rj = fma(-alpha, sj, e[u]);
+                        vh[k] = isfinite(dzh[k]) ? rj / dzh[k] + ec[hown[k]] : 0.0;
+                    }
+                }
+            }
+        }
+        __syncthreads();
+        // own rows: p = z_o + beta*p, s = w + beta*s, x += alpha*p, r -= alpha*s
+#pragma unroll
+        for (int k = 0; k < RMAX; ++k) {
+            const int i = row_of(k);
+            if (i < 0) continue;
+            const double zo = r[k] / dd[k] + s_ecp;
+            p[k] = fr[k] ? fma(beta, p[k], zo) : 0.0;
+            s[k] = fma(beta, s[k], w[k]);
+            if (fr[k]) D.pres[i] = fma(alpha, p[k], D.pres[i]);
+            r[k] = fma(-alpha, s[k], r[k]);
+            rb[pn][i] = r[k];
+            sb[pn][i] = s[k];
+        }
+        offdiag_all(off);
+        Acc6 a6{0.0, 0.0, 0.0, 0.0, 0.0};
+#pragma unroll
+        for (int k = 0; k < RMAX; ++k) {
+            const int i = row_of(k);
+            if (i < 0) continue;
+            const double zi = fr[k] ? r[k] / dd[k] + ec[s_own] : 0.0;
+            w[k] = fr[k] ? fma(D.pdiag[i], zi, off[k]) : 0.0;
+            wb[pn][i] = w[k];
+            if (fr[k]) {
+                if (!isfinite(r[k])) a6.flag = 1.0;
+                a6.a = fma(r[k], zi, a6.a);
+                a6.b = fma(zi, w[k], a6.b);
+                a6.c = fma(r[k], r[k], a6.c);
+                a6.mx = fmax(a6.mx, fabs(r[k]));
+            }
+        }
+        xs = 0.0;
+#pragma unroll
+        for (int k = 0; k < RMAX; ++k) xs += w[k];
+        t = Acc6{0.0, 0.0, 0.0, 0.0, 0.0};
+        if (!grid_allreduce3g<NT>(a6, xs, D, g, phase, t, cw)) return;
+        ++phase;
+        if (threadIdx.x == 0) s_ecp = ec[s_own];
         fin = sqrt(t.c);
         mx = t.mx;
         rel = fin / init;
@@ -1425,6 +1809,60 @@ __global__ void __launch_bounds__(NT, NT >= 512 ? 1 : 2) k_pcg32m(PcgDev D)
     if (!conv && b == 0 && threadIdx.x == 0) set_status(seg_status(D, g), 2, ST_PCG, it, R_PCG_MAXIT);
 }
 
+// ------------------------------------------------- two-level set-up kernels
+// Aggregated operator P^T A P of the free rows: one warp per nonzero (I, J)
+// block, summing its entries (coefficient slots, or the diagonal of row
+// -e-1) lane-strided and then by a fixed shuffle tree.
+__global__ void k_coarse_blocks(int npairs, const int* pair_ptr, const int2* pair_ij, const int* ent,
+                                const double* val, const double* pdiag_pos, int G, double* ac)
+{
+    const int q = (int)((blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5);
+    const int lane = threadIdx.x & 31;
+    if (q >= npairs) return;
+    double s = 0.0;
+    for (int k = pair_ptr[q] + lane; k < pair_ptr[q + 1]; k += 32) {
+        const int e = ent[k];
+        s += e >= 0 ? val[e] : pdiag_pos[-e - 1];
+    }
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+    if (lane == 0) ac[(size_t)pair_ij[q].x * G + pair_ij[q].y] = s;
+}
+
+// In-place Gauss-Jordan inverse of the SPD coarse operator in shared memory
+// (one CTA).  An aggregate without free rows has an empty row and column;
+// it gets a unit diagonal and stays decoupled.
+__global__ void __launch_bounds__(512) k_coarse_invert(int G, double* ac)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    double* a = reinterpret_cast<double*>(smem_raw);
+    double* rowk = a + (size_t)G * G;
+    double* colk = rowk + G;
+    for (int t = threadIdx.x; t < G * G; t += blockDim.x) a[t] = ac[t];
+    __syncthreads();
+    for (int t = threadIdx.x; t < G; t += blockDim.x)
+        if (a[(size_t)t * G + t] == 0.0) a[(size_t)t * G + t] = 1.0;
+    for (int k = 0; k < G; ++k) {
+        __syncthreads();
+        for (int t = threadIdx.x; t < G; t += blockDim.x) {
+            rowk[t] = a[(size_t)k * G + t];
+            colk[t] = a[(size_t)t * G + k];
+        }
+        __syncthreads();
+        const double pinv = 1.0 / rowk[k];
+        for (int t = threadIdx.x; t < G * G; t += blockDim.x) {
+            const int i = t / G, j = t % G;
+            double v;
+            if (i == k && j == k) v = pinv;
+            else if (i == k) v = rowk[j] * pinv;
+            else if (j == k) v = -colk[i] * pinv;
+            else v = a[t] - colk[i] * rowk[j] * pinv;
+            a[t] = v;
+        }
+    }
+    __syncthreads();
+    for (int t = threadIdx.x; t < G * G; t += blockDim.x) ac[t] = a[t];
+}
+
 // Self-test of the bounded device wait: CTA 0 leaves without arriving, so the
 // other CTAs' barrier waits can only end by running out of their spin limit.
 __global__ void k_barrier_selftest(unsigned* bar, DevStatus* st)
@@ -1474,6 +1912,13 @@ const void* fn_mixed(int rmax)
          : rmax == 4 ? reinterpret_cast<const void*>(k_pcg32m<4, BATCH, NT>)
                      : reinterpret_cast<const void*>(k_pcg32m<8, BATCH, NT>);
 }
+const void* fn_twolevel(int rmax)
+{
+    return rmax == 1 ? reinterpret_cast<const void*>(k_pcg64d<1>)
+         : rmax == 2 ? reinterpret_cast<const void*>(k_pcg64d<2>)
+         : rmax == 4 ? reinterpret_cast<const void*>(k_pcg64d<4>)
+                     : reinterpret_cast<const void*>(k_pcg64d<8>);
+}
 const void* fn_cgcg_single(int rmax, int nt) { return nt == 256 ? fn_cgcg<false, 256>(rmax) : fn_cgcg<false, 512>(rmax); }
 const void* fn_mixed_single(int rmax, int nt) { return nt == 256 ? fn_mixed<false, 256>(rmax) : fn_mixed<false, 512>(rmax); }
 
@@ -1483,8 +1928,103 @@ constexpr int BATCH_THREADS = 256;
 
 }  // namespace
 
+void PcgEngine::build_coarse(const HostModel& m, const std::vector<int>& colp)
+{
+    const int G = nblocks;
+    const PressurePattern& P = m.pat;
+    if (G > 160) return;   // the inverse must fit one CTA's shared memory
+    std::vector<int> cta_of_slice(static_cast<size_t>(nslices), 0);
+    for (int b = 0; b < G; ++b) {
+        const int sb = static_cast<int>(static_cast<long long>(b) * nslices / G);
+        const int se = static_cast<int>(static_cast<long long>(b + 1) * nslices / G);
+        for (int q = sb; q < se; ++q) cta_of_slice[static_cast<size_t>(q)] = b;
+    }
+    std::vector<char> fixed(static_cast<size_t>(N), 0), freep(static_cast<size_t>(NP), 0);
+    for (int v : m.bc_list) fixed[static_cast<size_t>(v - 1)] = 1;
+    for (int pos = 0; pos < NP; ++pos) {
+        const int node = P.row_node[static_cast<size_t>(pos)];
+        freep[static_cast<size_t>(pos)] = node >= 0 && m.tf[static_cast<size_t>(node)] && !fixed[static_cast<size_t>(node)];
+    }
+    // entries of every nonzero block (I, J) of P^T A P, ascending
+    std::vector<std::vector<int>> blocks(static_cast<size_t>(G) * G);
+    for (int q = 0; q < nslices; ++q) {
+        const int I = cta_of_slice[static_cast<size_t>(q)];
+        for (int lane = 0; lane < 32; ++lane) {
+            const int pos = q * 32 + lane;
+            if (!freep[static_cast<size_t>(pos)]) continue;
+            blocks[static_cast<size_t>(I) * G + I].push_back(-(pos + 1));
+            for (int k = 0; k < P.slice_w[static_cast<size_t>(q)]; ++k) {
+                const long long t = P.slice_off[static_cast<size_t>(q)] + lane + 32LL * k;
+                const int c = colp[static_cast<size_t>(t)];
+                if (!freep[static_cast<size_t>(c)]) continue;
+                blocks[static_cast<size_t>(I) * G + cta_of_slice[static_cast<size_t>(c / 32)]].push_back(static_cast<int>(t));
+            }
+        }
+    }
+    std::vector<int> ptr(1, 0), ent;
+    std::vector<int2> ij;
+    for (int I = 0; I < G; ++I)
+        for (int J = 0; J < G; ++J) {
+            auto& v = blocks[static_cast<size_t>(I) * G + J];
+            if (v.empty()) continue;
+            std::sort(v.begin(), v.end());
+            ent.insert(ent.end(), v.begin(), v.end());
+            ptr.push_back(static_cast<int>(ent.size()));
+            ij.push_back(make_int2(I, J));
+        }
+    // each CTA's neighbour list: itself and the owners of its halo entries
+    std::vector<int> nptr(1, 0), nids;
+    std::vector<unsigned char> hown(h_hidx.size(), 0);
+    int nmax = 0;
+    for (int b = 0; b < G; ++b) {
+        std::vector<int> l(1, b);
+        for (int k = h_hptr[static_cast<size_t>(b)]; k < h_hptr[static_cast<size_t>(b) + 1]; ++k)
+            l.push_back(cta_of_slice[static_cast<size_t>(h_hidx[static_cast<size_t>(k)] / 32)]);
+        std::sort(l.begin(), l.end());
+        l.erase(std::unique(l.begin(), l.end()), l.end());
+        if (l.size() > 255) return;
+        for (int k = h_hptr[static_cast<size_t>(b)]; k < h_hptr[static_cast<size_t>(b) + 1]; ++k) {
+            const int o = cta_of_slice[static_cast<size_t>(h_hidx[static_cast<size_t>(k)] / 32)];
+            hown[static_cast<size_t>(k)] = static_cast<unsigned char>(std::lower_bound(l.begin(), l.end(), o) - l.begin());
+        }
+        nids.insert(nids.end(), l.begin(), l.end());
+        nptr.push_back(static_cast<int>(nids.size()));
+        nmax = std::max(nmax, static_cast<int>(l.size()));
+    }
+    const size_t base = (halo_smem + 15) & ~static_cast<size_t>(15);
+    const size_t smem = base + (static_cast<size_t>(nmax) * G + 3 * static_cast<size_t>(G) + nmax) * 8 +
+                        static_cast<size_t>(dev_halo_max) + 16;
+    const size_t ismem = (static_cast<size_t>(G) * G + 2 * static_cast<size_t>(G)) * 8;
+    const void* fn = fn_twolevel(rmax);
+    int per = 0;
+    if (smem > 220 * 1024 || ismem > 220 * 1024 || raise_smem_limit(fn, smem) != cudaSuccess ||
+        raise_smem_limit(reinterpret_cast<const void*>(k_coarse_invert), ismem) != cudaSuccess ||
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, fn, 512, smem) != cudaSuccess || per * sms_ < G) {
+        cudaGetLastError();
+        return;
+    }
+    npairs = static_cast<int>(ij.size());
+    d_pair_ptr = dalloc<int>(ptr.size());
+    d_pair_ij = dalloc<int2>(ij.size());
+    d_pair_ent = dalloc<int>(ent.size());
+    d_ac = dalloc<double>(static_cast<size_t>(G) * G);
+    d_nbr_ptr = dalloc<int>(nptr.size());
+    d_nbr_ids = dalloc<int>(nids.size());
+    d_hown = dalloc<unsigned char>(hown.size());
+    CUDA_OK(cudaMemcpy(d_pair_ptr, ptr.data(), ptr.size() * sizeof(int), cudaMemcpyHostToDevice));
+    CUDA_OK(cudaMemcpy(d_pair_ij, ij.data(), ij.size() * sizeof(int2), cudaMemcpyHostToDevice));
+    CUDA_OK(cudaMemcpy(d_pair_ent, ent.data(), ent.size() * sizeof(int), cudaMemcpyHostToDevice));
+    CUDA_OK(cudaMemcpy(d_nbr_ptr, nptr.data(), nptr.size() * sizeof(int), cudaMemcpyHostToDevice));
+    CUDA_OK(cudaMemcpy(d_nbr_ids, nids.data(), nids.size() * sizeof(int), cudaMemcpyHostToDevice));
+    if (!hown.empty()) CUDA_OK(cudaMemcpy(d_hown, hown.data(), hown.size(), cudaMemcpyHostToDevice));
+    cdev = CoarseDev{G, nmax, d_nbr_ptr, d_nbr_ids, d_hown, d_ac};
+    coarse_smem = smem;
+    coarse_ismem = ismem;
+    coarse = true;
+}
+
 void PcgEngine::init(const HostModel& m, const uint8_t* nflag, const double* pfix, DevStatus* status,
-                     int device, int blocks_override, bool mixed_mode, int kernel_choice)
+                     int device, int blocks_override, bool mixed_mode, int kernel_choice, bool two_level)
 {
     N = m.N;
     E = m.E;
@@ -1533,6 +2073,7 @@ void PcgEngine::init(const HostModel& m, const uint8_t* nflag, const double* pfi
 
     int sms = 0;
     CUDA_OK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
+    sms_ = sms;
     // Register-resident kernel when every thread's rows fit its register
     // arrays; otherwise the kernel that keeps the vectors in global memory.
     auto grid_for = [&](const void* fn) {
@@ -1607,6 +2148,8 @@ void PcgEngine::init(const HostModel& m, const uint8_t* nflag, const double* pfi
             if (!lcol.empty()) CUDA_OK(cudaMemcpy(d_lcol, lcol.data(), lcol.size() * sizeof(unsigned short), cudaMemcpyHostToDevice));
             dev_halo_max = hmax;
             dev_slot_max = static_cast<int>(smax);
+            h_hptr = hptr;
+            h_hidx = hidx;
             if (mixed && want == 4) {
                 const void* mc[4] = {fn_mixed_single(1, nt), fn_mixed_single(2, nt), fn_mixed_single(4, nt),
                                      fn_mixed_single(8, nt)};
@@ -1632,6 +2175,7 @@ void PcgEngine::init(const HostModel& m, const uint8_t* nflag, const double* pfi
             if ((per_cta + PCG_WARPS - 1) / PCG_WARPS <= rm[c]) { rmax = rm[c]; nblocks = g; variant = 2; break; }
         }
     }
+    if (two_level && variant == 4 && nthreads == 512 && !mixed_ok) build_coarse(m, colp);
     d_part = dalloc<double>(static_cast<size_t>(nblocks) * 16);
     d_bar = dalloc<unsigned>(4);
     d_out = dalloc<CgOut>(1);
@@ -1657,8 +2201,11 @@ void PcgEngine::release()
 {
     void* ptrs[] = {d_slice_off, d_slice_w, d_col, d_cptr, d_cent, d_val, d_val32, d_r, d_z, d_pA,
                     d_pB, d_q, d_f32, d_part, d_bar, d_out, d_halo_ptr, d_halo_idx, d_lcol, d_row_node,
-                    d_xp, d_bp, d_dp, d_fp};
+                    d_xp, d_bp, d_dp, d_fp, d_pair_ptr, d_pair_ij, d_pair_ent, d_ac, d_nbr_ptr, d_nbr_ids, d_hown};
     for (void* p : ptrs) if (p) cudaFree(p);
+    d_pair_ptr = nullptr; d_pair_ij = nullptr; d_pair_ent = nullptr; d_ac = nullptr;
+    d_nbr_ptr = nullptr; d_nbr_ids = nullptr; d_hown = nullptr;
+    coarse = false;
     d_slice_off = nullptr; d_slice_w = nullptr; d_col = nullptr; d_cptr = nullptr; d_cent = nullptr;
     d_val = nullptr; d_val32 = nullptr; d_r = d_z = d_pA = d_pB = d_q = nullptr; d_f32 = nullptr;
     d_part = nullptr; d_bar = nullptr; d_out = nullptr;
@@ -1721,8 +2268,20 @@ cbs3d_status PcgEngine::solve(double* pres, double* rhs1, double* pdiag, int pre
         fn = fn_cgcg_single(rmax, nthreads);
         smem = halo_smem;
     }
+    CoarseDev C = cdev;
+    void* args2[] = {&D, &C};
+    if (coarse) {
+        // the aggregated operator of this solve and its inverse
+        const int G = nblocks;
+        CUDA_OK(cudaMemsetAsync(d_ac, 0, static_cast<size_t>(G) * G * sizeof(double), st));
+        k_coarse_blocks<<<static_cast<unsigned>((static_cast<long long>(npairs) * 32 + 255) / 256), 256, 0, st>>>(
+            npairs, d_pair_ptr, d_pair_ij, d_pair_ent, d_val, d_dp, G, d_ac);
+        k_coarse_invert<<<1, 512, coarse_ismem, st>>>(G, d_ac);
+        fn = fn_twolevel(rmax);
+        smem = coarse_smem;
+    }
     if (ev0) CUDA_OK(cudaEventRecord(ev0, st));
-    CUDA_OK(cudaLaunchCooperativeKernel(fn, dim3(nblocks), dim3(nthreads), args, smem, st));
+    CUDA_OK(cudaLaunchCooperativeKernel(fn, dim3(nblocks), dim3(nthreads), coarse ? args2 : args, smem, st));
     if (ev1) CUDA_OK(cudaEventRecord(ev1, st));
     k_perm_out<<<(NP + 255) / 256, 256, 0, st>>>(D, d_xp, pres);
     if (sync) CUDA_OK(cudaStreamSynchronize(st));

@@ -66,14 +66,29 @@ struct PcgDev {
     const PcgInst* inst;         // batched launch: instance descriptors (else null)
 };
 
+// Two-level preconditioner data of one launch: the coarse space is one
+// aggregate per CTA (its free rows); ainv is the inverse of the aggregated
+// operator P^T A P, nbr_ptr/nbr_ids each CTA's own and halo-owner CTAs, and
+// hown the position of every halo entry's owner in its CTA's list.
+struct CoarseDev {
+    int G;
+    int nbr_max;
+    const int* nbr_ptr;
+    const int* nbr_ids;
+    const unsigned char* hown;
+    const double* ainv;
+};
+
 // Owns the device copies of the pattern and the PCG work vectors.
 class PcgEngine {
 public:
     // kernel_choice: 0 automatic (4, else 3, else 2, else 1), 1 vectors in global memory,
     // 2 register-resident rows, 3 with the halo staged in shared memory,
     // 4 as 3 with one grid synchronisation per iteration (Chronopoulos-Gear)
+    // two_level: Jacobi plus a coarse correction on one aggregate per CTA
+    // (large meshes with the single-reduction kernel; else plain Jacobi)
     void init(const HostModel& m, const uint8_t* d_nflag, const double* d_pfix, DevStatus* d_status,
-              int device, int blocks_override, bool mixed, int kernel_choice = 0);
+              int device, int blocks_override, bool mixed, int kernel_choice = 0, bool two_level = false);
     void release();
     // ELL values from gstifE*delte (step path) or from a caller's gstif[6E].
     void assemble_from_state(const DevState& S, cudaStream_t st);
@@ -84,7 +99,7 @@ public:
                        int max_iter, double rel_tol, double abs_tol, cudaStream_t st, bool sync,
                        cudaEvent_t ev0 = nullptr, cudaEvent_t ev1 = nullptr);
     // impose, permute in, solver, permute out
-    int launches_per_solve() const { return 4; }
+    int launches_per_solve() const { return coarse ? 6 : 4; }
     cbs3d_status read_result(cbs3d_cg_result& r, cudaStream_t st);
     // y = A x with the assembled operator (identity rows on fixed nodes).
     void multiply(const double* d_pdiag, const double* d_x, double* d_y, cudaStream_t st);
@@ -92,6 +107,16 @@ public:
     bool mixed = false;
     int rmax = 0;            // rows per thread of the register-resident kernels (0: global kernel)
     int nthreads = 512;      // CTA size of the persistent kernel
+    bool coarse = false;     // two-level preconditioner in use
+    size_t coarse_smem = 0, coarse_ismem = 0;
+    int npairs = 0, sms_ = 0;
+    int *d_pair_ptr = nullptr, *d_pair_ent = nullptr, *d_nbr_ptr = nullptr, *d_nbr_ids = nullptr;
+    int2* d_pair_ij = nullptr;
+    double* d_ac = nullptr;
+    unsigned char* d_hown = nullptr;
+    CoarseDev cdev{};
+    std::vector<int> h_hptr, h_hidx;
+    void build_coarse(const HostModel& m, const std::vector<int>& colp);
     int variant = 1;         // 1 global vectors, 2 register rows, 3 + shared-memory halo, 4 + one sync per iteration
     size_t halo_smem = 0;    // dynamic shared memory of the halo kernel
     size_t mixed_smem = 0;   // dynamic shared memory of the mixed-precision kernel

@@ -100,6 +100,9 @@ typedef struct cbs3d_options {
                                 3 shared-memory halo, 4 halo + one grid sync per iteration */
     int case_cache;          /* cbs3d_create_from_case: keep the parsed case in <case>.cbscache
                                 (keyed by every source file's size and time) and reuse it */
+    int pcg_two_level;       /* extension: Jacobi plus a coarse correction on one aggregate of rows
+                                per CTA (the aggregated operator is rebuilt and inverted every solve);
+                                same stopping test, far fewer iterations; large meshes only */
 } cbs3d_options;
 
 /* Mirrors ConjugateGradient::Result (include/cbs/linalg/ConjugateGradient.hpp:36-68).
@@ -132,7 +135,7 @@ typedef struct cbs3d_step_stats {
     double pcg_bytes_per_iter; /* bytes one PCG iteration of the selected kernel moves */
     int pcg_kernel;          /* PCG kernel in use: 1 global vectors, 2 register rows,
                                 3 shared-memory halo, 4 single-reduction (CG-CG),
-                                5 mixed FP32/FP64 */
+                                5 mixed FP32/FP64, 6 two-level (CG-CG + coarse correction) */
 } cbs3d_step_stats;
 
 typedef struct cbs3d_ctx cbs3d_ctx;
