@@ -12,10 +12,13 @@ and node data, far more than the 126 MB L2, so no flush is inserted.
   python bench.py [--gpus N] [--steps K] [--warmup W] [--precision both|fp64|mixed]
   python bench.py --impl reference ...   # the reference solver on the host cores
 
-`value` is the FP64 engine (the drop-in for the reference's FP64 path); with
---precision both (the default) the same line carries the mixed engine (FP32
-inner PCG, FP64 defect correction) under "mixed": its steps/s, and its
-relative L2 error on u and p against the FP64 engine after the same steps.
+`value` is the FP64 engine with the reference's Jacobi-PCG (the drop-in for
+the reference's FP64 path); with --precision both (the default) the same
+line carries the mixed engine (FP32 inner PCG, FP64 defect correction) under
+"mixed" and the FP64 engine with the two-level preconditioner (Jacobi plus a
+per-CTA coarse correction, same stopping test) under "two_level": their
+steps/s and relative L2 errors on u and p against the Jacobi FP64 engine
+after the same steps.
 
 Roofline of the PCG kernel: algorithmic bytes per iteration are the
 element-by-element operator's traffic, 64*E_f + 73*N in FP64 and
@@ -300,6 +303,20 @@ def arm_gpu(args):
     pcg_share = st.pcg_seconds / st.gpu_seconds if st.gpu_seconds > 0 else None
     ctx.close()
 
+    # the two-level preconditioner (extension): FP64, same stopping test
+    two = None
+    if args.precision in ("both", "fp64"):
+        tctx = gpu.Context(case, precision=gpu.FP64, device=local, use_graph=False, time_pcg=True, two_level=True)
+        twarm, tst, tsec, _ = timed_run(args, tctx, dist)
+        ut, pt, _ = tctx.fields()
+        two = {"value": ws * args.steps / tsec, "unit": "steps/s", "ms_per_step": 1e3 * tsec / args.steps,
+               "speedup_vs_fp64": (ws * args.steps / tsec) / value, "pcg_kernel": int(tst.pcg_kernel),
+               "rel_l2_u_vs_fp64": float(np.linalg.norm(ut - u0) / np.linalg.norm(u0)),
+               "rel_l2_p_vs_fp64": float(np.linalg.norm(pt - p0) / np.linalg.norm(p0)),
+               "pcg_iterations_per_step": (tst.cg_iterations_total - twarm.cg_iterations_total) / args.steps}
+        two["gpu_launches"] = int(tst.kernel_launches)
+        tctx.close()
+
     mixed = None
     if args.precision == "both":
         mctx = gpu.Context(case, precision=gpu.MIXED, device=local, use_graph=False, time_pcg=True)
@@ -311,7 +328,7 @@ def arm_gpu(args):
                  "rel_l2_p_vs_fp64": float(np.linalg.norm(pm - p0) / np.linalg.norm(p0)),
                  "pcg_iterations_per_step": (mst.cg_iterations_total - mwarm.cg_iterations_total) / args.steps,
                  "roofline": roofline(mst, mwarm, nelem_fluid, N, True, args.n)}
-        launches += int(mst.kernel_launches)
+        mixed["gpu_launches"] = int(mst.kernel_launches)
         mctx.close()
 
     cpu = None
@@ -334,6 +351,8 @@ def arm_gpu(args):
         }
         if mixed is not None:
             line["mixed"] = mixed
+        if two is not None:
+            line["two_level"] = two
         print(json.dumps(line))
     if dist is not None:
         barrier(dist)

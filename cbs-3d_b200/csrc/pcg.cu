@@ -1810,53 +1810,59 @@ __global__ void __launch_bounds__(NT, NT >= 512 ? 1 : 2) k_pcg32m(PcgDev D)
 }
 
 // ------------------------------------------------- two-level set-up kernels
-// Aggregated operator P^T A P of the free rows: one warp per nonzero (I, J)
-// block, summing its entries (coefficient slots, or the diagonal of row
-// -e-1) lane-strided and then by a fixed shuffle tree.
-__global__ void k_coarse_blocks(int npairs, const int* pair_ptr, const int2* pair_ij, const int* ent,
-                                const double* val, const double* pdiag_pos, int G, double* ac)
+// Aggregated operator P^T A P of the free rows: one CTA per nonzero (I, J)
+// block; thread t sums entries t, t+T, ... (coefficient slots, or the
+// diagonal of row -e-1), then warps and the CTA reduce in a fixed order.
+__global__ void __launch_bounds__(256) k_coarse_blocks(const int* pair_ptr, const int2* pair_ij, const int* ent,
+                                                       const double* val, const double* pdiag_pos, int G, double* ac)
 {
-    const int q = (int)((blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5);
-    const int lane = threadIdx.x & 31;
-    if (q >= npairs) return;
+    __shared__ double sm[8];
+    const int q = blockIdx.x;
     double s = 0.0;
-    for (int k = pair_ptr[q] + lane; k < pair_ptr[q + 1]; k += 32) {
+    for (int k = pair_ptr[q] + threadIdx.x; k < pair_ptr[q + 1]; k += 256) {
         const int e = ent[k];
         s += e >= 0 ? val[e] : pdiag_pos[-e - 1];
     }
     for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
-    if (lane == 0) ac[(size_t)pair_ij[q].x * G + pair_ij[q].y] = s;
+    if ((threadIdx.x & 31) == 0) sm[threadIdx.x >> 5] = s;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double t = 0.0;
+        for (int w = 0; w < 8; ++w) t += sm[w];
+        ac[(size_t)pair_ij[q].x * G + pair_ij[q].y] = t;
+    }
 }
 
 // In-place Gauss-Jordan inverse of the SPD coarse operator in shared memory
-// (one CTA).  An aggregate without free rows has an empty row and column;
-// it gets a unit diagonal and stays decoupled.
+// (one CTA; warps take rows, lanes columns).  An aggregate without free rows
+// has an empty row and column; it gets a unit diagonal and stays decoupled.
 __global__ void __launch_bounds__(512) k_coarse_invert(int G, double* ac)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     double* a = reinterpret_cast<double*>(smem_raw);
     double* rowk = a + (size_t)G * G;
     double* colk = rowk + G;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
     for (int t = threadIdx.x; t < G * G; t += blockDim.x) a[t] = ac[t];
     __syncthreads();
     for (int t = threadIdx.x; t < G; t += blockDim.x)
         if (a[(size_t)t * G + t] == 0.0) a[(size_t)t * G + t] = 1.0;
     for (int k = 0; k < G; ++k) {
         __syncthreads();
+        const double pinv = 1.0 / a[(size_t)k * G + k];
         for (int t = threadIdx.x; t < G; t += blockDim.x) {
-            rowk[t] = a[(size_t)k * G + t];
+            rowk[t] = a[(size_t)k * G + t] * pinv;   // new row k (its pivot entry fixed below)
             colk[t] = a[(size_t)t * G + k];
         }
         __syncthreads();
-        const double pinv = 1.0 / rowk[k];
-        for (int t = threadIdx.x; t < G * G; t += blockDim.x) {
-            const int i = t / G, j = t % G;
-            double v;
-            if (i == k && j == k) v = pinv;
-            else if (i == k) v = rowk[j] * pinv;
-            else if (j == k) v = -colk[i] * pinv;
-            else v = a[t] - colk[i] * rowk[j] * pinv;
-            a[t] = v;
+        for (int i = warp; i < G; i += nw) {
+            double* ai = a + (size_t)i * G;
+            if (i == k) {
+                for (int j = lane; j < G; j += 32) ai[j] = (j == k) ? pinv : rowk[j];
+            } else {
+                const double ci = colk[i];
+                for (int j = lane; j < G; j += 32) ai[j] = (j == k) ? -ci * pinv : fma(-ci, rowk[j], ai[j]);
+            }
         }
     }
     __syncthreads();
@@ -2274,8 +2280,8 @@ cbs3d_status PcgEngine::solve(double* pres, double* rhs1, double* pdiag, int pre
         // the aggregated operator of this solve and its inverse
         const int G = nblocks;
         CUDA_OK(cudaMemsetAsync(d_ac, 0, static_cast<size_t>(G) * G * sizeof(double), st));
-        k_coarse_blocks<<<static_cast<unsigned>((static_cast<long long>(npairs) * 32 + 255) / 256), 256, 0, st>>>(
-            npairs, d_pair_ptr, d_pair_ij, d_pair_ent, d_val, d_dp, G, d_ac);
+        k_coarse_blocks<<<static_cast<unsigned>(npairs), 256, 0, st>>>(d_pair_ptr, d_pair_ij, d_pair_ent, d_val, d_dp, G,
+                                                                      d_ac);
         k_coarse_invert<<<1, 512, coarse_ismem, st>>>(G, d_ac);
         fn = fn_twolevel(rmax);
         smem = coarse_smem;
