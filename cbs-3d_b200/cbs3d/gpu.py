@@ -171,6 +171,8 @@ def lib():
         L.cbs3d_write_residual_rows.restype = _i
         L.cbs3d_step_history.argtypes = [vp, _i, _i, vp]
         L.cbs3d_step_history.restype = _i
+        L.cbs3d_solve_pressure.argtypes = [vp, vp, vp, vp, vp, ctypes.POINTER(CGResult)]
+        L.cbs3d_solve_pressure.restype = _i
         L.cbs3d_set_body_force.argtypes = [vp, vp]
         L.cbs3d_objective_run.argtypes = [vp, _i, vp, ctypes.POINTER(_d)]
         L.cbs3d_tlm_run.argtypes = [vp, _i, vp, vp, ctypes.POINTER(_d), ctypes.POINTER(_d)]
@@ -406,6 +408,18 @@ class Context:
         J = ctypes.c_double()
         self._check(lib().cbs3d_heat_adjoint_run(self.h, nsteps, every, _ptr(w), ctypes.byref(J), _ptr(g)))
         return J.value, g
+
+    def solve_pressure(self, gstif, pdiag, rhs1, pres):
+        """cbs3d_solve_pressure on copies: returns (pres, rhs1, pdiag, result dict)."""
+        g = np.ascontiguousarray(gstif, dtype=np.float64)
+        pd, r1, p = (np.array(a, dtype=np.float64) for a in (pdiag, rhs1, pres))
+        res = CGResult()
+        rc = lib().cbs3d_solve_pressure(self.h, _ptr(g), _ptr(pd), _ptr(r1), _ptr(p), ctypes.byref(res))
+        if rc != 0 and rc != 2:
+            self._check(rc)
+        out = res.as_dict()
+        out["status"] = rc
+        return p, r1, pd, out
 
     def pressure_multiply(self, x) -> np.ndarray:
         x = np.ascontiguousarray(x, dtype=np.float64)

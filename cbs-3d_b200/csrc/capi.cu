@@ -754,6 +754,39 @@ cbs3d_status cbs3d_run_stage(cbs3d_ctx* c, const char* stage)
     });
 }
 
+cbs3d_status cbs3d_solve_pressure(cbs3d_ctx* c, const double* gstif, double* pdiag, double* rhs1, double* pres,
+                                  cbs3d_cg_result* result)
+{
+    return guarded(c, [&] {
+        if (!gstif || !pdiag || !rhs1 || !pres) throw Error(CBS3D_INVALID_INPUT, "cbs3d_solve_pressure - null array");
+        if (c->batch_out) throw Error(CBS3D_INVALID_INPUT, "cbs3d_solve_pressure - context belongs to a batch");
+        const size_t E = c->m.E, N = c->m.N;
+        const cudaStream_t st = c->st;
+        double* dg = nullptr;
+        CUDA_OK(cudaMalloc(&dg, 6 * E * sizeof(double)));
+        struct Free { double* p; ~Free() { cudaFree(p); } } guard{dg};
+        CUDA_OK(cudaMemcpyAsync(dg, gstif, 6 * E * sizeof(double), cudaMemcpyHostToDevice, st));
+        CUDA_OK(cudaMemcpyAsync(c->S.pdiag, pdiag, N * sizeof(double), cudaMemcpyHostToDevice, st));
+        CUDA_OK(cudaMemcpyAsync(c->S.rhs1, rhs1, N * sizeof(double), cudaMemcpyHostToDevice, st));
+        CUDA_OK(cudaMemcpyAsync(c->S.pres, pres, N * sizeof(double), cudaMemcpyHostToDevice, st));
+        c->reset_status();
+        c->pcg.assemble_from_gstif(dg, st);
+        const cbs3d_params& P = c->m.p;
+        c->pcg.solve(c->S.pres, c->S.rhs1, c->S.pdiag, P.cg_preconditioner, P.cg_conv_test, P.cg_max_iter,
+                     P.relToler, P.absToler, st, false);
+        CUDA_OK(cudaMemcpyAsync(pres, c->S.pres, N * sizeof(double), cudaMemcpyDeviceToHost, st));
+        CUDA_OK(cudaMemcpyAsync(rhs1, c->S.rhs1, N * sizeof(double), cudaMemcpyDeviceToHost, st));
+        CUDA_OK(cudaMemcpyAsync(pdiag, c->S.pdiag, N * sizeof(double), cudaMemcpyDeviceToHost, st));
+        cbs3d_cg_result r{};
+        const cbs3d_status conv = c->pcg.read_result(r, st);
+        DevStatus ds{};
+        CUDA_OK(cudaMemcpy(&ds, c->S.status, sizeof ds, cudaMemcpyDeviceToHost));
+        if (result) *result = r;
+        if (ds.code != 0 && ds.code != CBS3D_NOT_CONVERGED) throw Error(static_cast<cbs3d_status>(ds.code), reason_text(ds));
+        if (conv != CBS3D_OK) throw Error(conv, "Steps::step2SemiImplicit - pressure solver failed to converge");
+    });
+}
+
 cbs3d_status cbs3d_pressure_multiply(cbs3d_ctx* c, const double* x, double* y)
 {
     return guarded(c, [&] {

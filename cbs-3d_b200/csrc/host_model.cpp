@@ -684,6 +684,46 @@ std::vector<int> locality_order(const double* coord, int N)
     return ord;
 }
 
+// Coordinate-free locality order: breadth-first (Cuthill-McKee) levels from a
+// pseudo-peripheral node of each connected component, neighbours visited in
+// element order, so consecutive rows are near each other in the mesh.
+std::vector<int> graph_order(const std::vector<int>& intma, const std::vector<int>& n2e_ptr,
+                             const std::vector<int>& n2e, int N)
+{
+    const size_t Ns = static_cast<size_t>(N);
+    std::vector<int> order, level(Ns, -1), q;
+    order.reserve(Ns);
+    auto bfs = [&](int start, std::vector<int>& out, std::vector<int>& lev) {
+        out.clear();
+        out.push_back(start);
+        lev[static_cast<size_t>(start)] = 0;
+        for (size_t h = 0; h < out.size(); ++h) {
+            const int i = out[h];
+            for (int k = n2e_ptr[static_cast<size_t>(i)]; k < n2e_ptr[static_cast<size_t>(i) + 1]; ++k) {
+                const size_t e = static_cast<size_t>(n2e[static_cast<size_t>(k)] >> 2);
+                for (int a = 0; a < 4; ++a) {
+                    const int j = intma[4 * e + a] - 1;
+                    if (lev[static_cast<size_t>(j)] < 0) {
+                        lev[static_cast<size_t>(j)] = lev[static_cast<size_t>(i)] + 1;
+                        out.push_back(j);
+                    }
+                }
+            }
+        }
+    };
+    std::vector<int> seen(Ns, 0), tmp_level(Ns, -1), comp;
+    for (int s0 = 0; s0 < N; ++s0) {
+        if (seen[static_cast<size_t>(s0)]) continue;
+        // the last node reached from s0 starts the ordering sweep
+        bfs(s0, comp, tmp_level);
+        const int far = comp.back();
+        for (int v : comp) tmp_level[static_cast<size_t>(v)] = -1;
+        bfs(far, q, level);
+        for (int v : q) { seen[static_cast<size_t>(v)] = 1; order.push_back(v); }
+    }
+    return order;
+}
+
 // Pattern of the assembled pressure operator (see PressurePattern); row
 // position p holds node order[p].
 void build_pressure_pattern(const std::vector<int>& intma, const std::vector<int>& mat, int N,
@@ -693,7 +733,7 @@ void build_pressure_pattern(const std::vector<int>& intma, const std::vector<int
     const size_t Ns = static_cast<size_t>(N);
     static const int PAIR[4][4] = {{-1, 0, 1, 2}, {0, -1, 3, 4}, {1, 3, -1, 5}, {2, 4, 5, -1}};
     pat = PressurePattern{};
-    const std::vector<int> order = locality_order(coord, N);
+    const std::vector<int> order = coord ? locality_order(coord, N) : graph_order(intma, n2e_ptr, n2e, N);
     pat.nslices = (N + 31) / 32;
     pat.row_node.assign(static_cast<size_t>(pat.nslices) * 32, -1);
     for (size_t q = 0; q < Ns; ++q) pat.row_node[q] = order[q];

@@ -199,6 +199,16 @@ cbs3d_status cbs3d_set_array(cbs3d_ctx* ctx, const char* name, const void* host,
  * step1, step2_rhs, solve_pressure, step3, step4, convergence. */
 cbs3d_status cbs3d_run_stage(cbs3d_ctx* ctx, const char* stage);
 
+/* The pressure-solver drop-in on a context (solver_opt=1 semantics of
+ * ConjugateGradient::solvePressure, src/linalg/ConjugateGradient.cpp:584-869,
+ * with the context's cg_* parameters): host arrays gstif[6*nelem] (pair
+ * order 12,13,14,23,24,34 per element), pdiag, rhs1 and pres[npoin]; pres is
+ * the initial guess and the solution, rhs1 and pdiag come back with the
+ * fixed and inactive rows imposed.  Returns CBS3D_NOT_CONVERGED (result
+ * filled) when the stopping test is not met. */
+cbs3d_status cbs3d_solve_pressure(cbs3d_ctx* ctx, const double* gstif, double* pdiag, double* rhs1, double* pres,
+                                  cbs3d_cg_result* result);
+
 /* y = A x with the context's current pressure operator
  * (MatrixVectorCalc::pressureMultiply, src/linalg/MatrixVectorCalc.cpp:125-205). */
 cbs3d_status cbs3d_pressure_multiply(cbs3d_ctx* ctx, const double* x, double* y);

@@ -142,6 +142,20 @@ def test_dropin_pressure_solver():
     assert bitwise(rhs1, z["ref_s5_rhs1"])
     assert bitwise(pdiag, z["ref_s5_pdiag"])
     assert abs(res["iterations"] - int(z["ref_s5_cg"][0])) <= 2
+
+
+def test_context_solve_pressure():
+    """cbs3d_solve_pressure: the drop-in on a context, same inputs and
+    side effects as the standalone solver."""
+    case, z = load_case(fixture_path("cav6j"))
+    c = _gpu().Context(case)
+    pres, rhs1, pdiag, res = c.solve_pressure(z["ref_s4_gstif"], z["ref_s4_pdiag_in"], z["ref_s4_rhs1"],
+                                              z["ref_s4_pres_in"])
+    assert res["status"] == 0 and res["converged"] == 1
+    assert rel_l2(pres, z["ref_s5_pres"]) <= PCG_TOL
+    assert bitwise(rhs1, z["ref_s5_rhs1"])
+    assert bitwise(pdiag, z["ref_s5_pdiag"])
+    assert abs(res["iterations"] - int(z["ref_s5_cg"][0])) <= 2
     assert abs(res["initial_l2"] - z["ref_s5_cg"][1]) <= 1e-12 * abs(z["ref_s5_cg"][1])
 
 
