@@ -147,3 +147,38 @@ def test_vtu_writer_layout(tmp_path):
     assert np.array_equal(v["mat_id"], np.r_[mat, np.full(NB, -1)])
     assert np.array_equal(v["cell_kind"], np.r_[np.full(E, 1), np.full(NB, 2)])
     assert np.array_equal(v["parent_element"][:E], np.arange(1, E + 1))
+
+
+def test_abi_rejects_bad_inputs_before_touching_a_device():
+    """Invalid sizes, connectivity and options are rejected on the host with
+    the reference's messages (no device is needed to see them)."""
+    from cbs3d import cases, gpu
+    L = gpu.lib()
+    c = cases.cavity(2, ntime=1)
+    mesh, par, keep = gpu._mesh_params(c)
+    opt = gpu.make_options()
+    h = ctypes.c_void_p()
+    err = ctypes.create_string_buffer(512)
+    bad = gpu.Mesh(0, c.mesh.npoin, c.mesh.nboun, mesh.intma, mesh.coord, mesh.bface, mesh.mat_elem)
+    assert L.cbs3d_create(ctypes.byref(bad), ctypes.byref(par), ctypes.byref(opt), ctypes.byref(h), err, 512) == 1
+    assert b"non-positive mesh size" in err.value
+    intma = c.mesh.intma.astype(np.int32).copy()
+    intma[0, 0] = c.mesh.npoin + 5
+    m2 = gpu.Mesh(c.mesh.nelem, c.mesh.npoin, c.mesh.nboun, gpu._ptr(intma), mesh.coord, mesh.bface, mesh.mat_elem)
+    assert L.cbs3d_create(ctypes.byref(m2), ctypes.byref(par), ctypes.byref(opt), ctypes.byref(h), err, 512) == 1
+    assert b"connectivity node out of range" in err.value
+    assert L.cbs3d_create(None, ctypes.byref(par), ctypes.byref(opt), ctypes.byref(h), err, 512) == 1
+    bo = gpu.BatchOptions()
+    L.cbs3d_default_batch_options(ctypes.byref(bo))
+    assert L.cbs3d_batch_create(0, None, None, ctypes.byref(bo), ctypes.byref(h), err, 512) == 1
+    pcg = ctypes.c_void_p()
+    assert L.cbs3d_pcg_create(c.mesh.nelem, c.mesh.npoin, gpu._ptr(intma), None, 0, None, None, None,
+                              ctypes.byref(pcg), err, 512) == 1
+    assert b"out of range" in err.value
+    # a fixed-pressure node outside the fluid
+    good = c.mesh.intma.astype(np.int32)
+    bl = np.array([c.mesh.npoin + 1], dtype=np.int32)
+    bv = np.zeros(1)
+    assert L.cbs3d_pcg_create(c.mesh.nelem, c.mesh.npoin, gpu._ptr(good), None, 1, gpu._ptr(bl), gpu._ptr(bv), None,
+                              ctypes.byref(pcg), err, 512) == 1
+    assert b"fixed pressure node out of range" in err.value
