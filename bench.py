@@ -53,12 +53,12 @@ N_HEX, RE, JITTER, SEED = 64, 400.0, 0.15, 1234
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=40)
+    ap.add_argument("--steps", type=int, default=200)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="gpu", choices=["gpu", "reference"])
     ap.add_argument("--precision", default="both", choices=["both", "fp64", "mixed"])
     ap.add_argument("--n", type=int, default=N_HEX, help="hexes per side")
-    ap.add_argument("--e2e-steps", type=int, default=3)
+    ap.add_argument("--e2e-steps", type=int, default=20)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--workload", default="cavity64", choices=["cavity64", "batch"],
                     help="batch: 48 seeded cavities of 10..40 hexes per side, Re 50..1000, batched step")
@@ -87,10 +87,16 @@ class ClockSampler:
         self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
         try:
             self.p = subprocess.Popen(["nvidia-smi", "-i", str(device), f"--query-gpu={self.Q}",
-                                       "--format=csv,noheader,nounits", "-lms", "200"],
+                                       "--format=csv,noheader,nounits", "-lms", "100"],
                                       stdout=self.f, stderr=subprocess.DEVNULL)
         except OSError:
             self.p = None
+            return
+        # nvidia-smi takes a few hundred ms to start: wait (at most 5 s) for its
+        # first sample so that the samples cover the timed region
+        t0 = time.time()
+        while time.time() - t0 < 5.0 and self.p.poll() is None and os.path.getsize(self.f.name) == 0:
+            time.sleep(0.02)
 
     def stop(self) -> dict:
         if self.p is None:

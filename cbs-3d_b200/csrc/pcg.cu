@@ -956,7 +956,7 @@ __global__ void __launch_bounds__(NT, NT >= 512 ? 1 : 2) k_pcg64c(PcgDev D)
     double* rb[2] = {D.r, D.r + N};
     double* wb[2] = {D.q, D.q + N};
     double* sb[2] = {D.pA, D.pB};
-    double* dz = D.z;   // free ? diagonal : +inf  (z = r / dz)
+    double* dz = D.z;   // free ? 1/diagonal : 0  (z = r * dz)
 
     double r[RMAX], p[RMAX], s[RMAX], w[RMAX], dd[RMAX];
     bool fr[RMAX];
@@ -974,7 +974,7 @@ __global__ void __launch_bounds__(NT, NT >= 512 ? 1 : 2) k_pcg64c(PcgDev D)
             wmax = wr[k] > wmax ? wr[k] : wmax;
         }
         r[k] = p[k] = s[k] = w[k] = 0.0;
-        dd[k] = __longlong_as_double(0x7ff0000000000000LL);
+        dd[k] = 0.0;   // reciprocal of the Jacobi diagonal; 0 off the free rows
         fr[k] = false;
     }
     constexpr int CH = (RMAX >= 8) ? 2 : (RMAX >= 4) ? 4 : 8;
@@ -1029,7 +1029,7 @@ __global__ void __launch_bounds__(NT, NT >= 512 ? 1 : 2) k_pcg64c(PcgDev D)
         if (fr[k]) {
             if (g.precond) {
                 if (!(isfinite(pd) && pd > 1.0e-30)) acc.flag = fmax(acc.flag, 1.0);
-                dd[k] = pd;
+                dd[k] = 1.0 / pd;
             } else {
                 dd[k] = 1.0;
             }
@@ -1065,7 +1065,7 @@ __global__ void __launch_bounds__(NT, NT >= 512 ? 1 : 2) k_pcg64c(PcgDev D)
 #pragma unroll
         for (int u = 0; u < 4; ++u) {
             const int k = k0 + u * NT;
-            if (k < nh) { dzh[k] = a[u]; vh[k] = c[u] / a[u]; }
+            if (k < nh) { dzh[k] = a[u]; vh[k] = c[u] * a[u]; }
         }
     }
     __syncthreads();
@@ -1075,7 +1075,7 @@ __global__ void __launch_bounds__(NT, NT >= 512 ? 1 : 2) k_pcg64c(PcgDev D)
     for (int k = 0; k < RMAX; ++k) {
         const int i = row[k];
         if (i < 0) continue;
-        const double zi = r[k] / dd[k];
+        const double zi = r[k] * dd[k];
         w[k] = fr[k] ? fma(D.pdiag[i], zi, off[k]) : 0.0;
         wb[0][i] = w[k];
         if (fr[k]) {
@@ -1119,7 +1119,7 @@ __global__ void __launch_bounds__(NT, NT >= 512 ? 1 : 2) k_pcg64c(PcgDev D)
                     if (k < nh) {
                         const double sj = fma(beta, a[u], c[u]);
                         const double rj = fma(-alpha, sj, e[u]);
-                        vh[k] = rj / dzh[k];
+                        vh[k] = rj * dzh[k];
                     }
                 }
             }
@@ -1130,7 +1130,7 @@ __global__ void __launch_bounds__(NT, NT >= 512 ? 1 : 2) k_pcg64c(PcgDev D)
         for (int k = 0; k < RMAX; ++k) {
             const int i = row[k];
             if (i < 0) continue;
-            const double zo = r[k] / dd[k];
+            const double zo = r[k] * dd[k];
             p[k] = fr[k] ? fma(beta, p[k], zo) : 0.0;
             s[k] = fma(beta, s[k], w[k]);
             if (fr[k]) D.pres[i] = fma(alpha, p[k], D.pres[i]);
@@ -1144,7 +1144,7 @@ __global__ void __launch_bounds__(NT, NT >= 512 ? 1 : 2) k_pcg64c(PcgDev D)
         for (int k = 0; k < RMAX; ++k) {
             const int i = row[k];
             if (i < 0) continue;
-            const double zi = r[k] / dd[k];
+            const double zi = r[k] * dd[k];
             w[k] = fr[k] ? fma(D.pdiag[i], zi, off[k]) : 0.0;
             wb[pn][i] = w[k];
             if (fr[k]) {
@@ -1234,7 +1234,7 @@ __global__ void __launch_bounds__(512, 1) k_pcg64d(PcgDev D, CoarseDev C)
     double* rb[2] = {D.r, D.r + N};
     double* wb[2] = {D.q, D.q + N};
     double* sb[2] = {D.pA, D.pB};
-    double* dz = D.z;   // free ? diagonal : +inf  (z = r / dz)
+    double* dz = D.z;   // free ? 1/diagonal : 0  (z = r * dz)
 
     // rows of this thread: slice s_beg + warp + NW*k, lane; their slot base
     // and width are re-read where needed (registers go to the coarse state)
@@ -1250,7 +1250,7 @@ __global__ void __launch_bounds__(512, 1) k_pcg64d(PcgDev D, CoarseDev C)
         const int wk = width_of(k);
         wmax = wk > wmax ? wk : wmax;
         r[k] = p[k] = s[k] = w[k] = 0.0;
-        dd[k] = __longlong_as_double(0x7ff0000000000000LL);
+        dd[k] = 0.0;   // reciprocal of the Jacobi diagonal; 0 off the free rows
         fr[k] = false;
     }
     constexpr int CH = (RMAX >= 8) ? 2 : (RMAX >= 4) ? 4 : 8;
@@ -1306,7 +1306,7 @@ __global__ void __launch_bounds__(512, 1) k_pcg64d(PcgDev D, CoarseDev C)
         if (fr[k]) {
             if (g.precond) {
                 if (!(isfinite(pd) && pd > 1.0e-30)) acc.flag = fmax(acc.flag, 1.0);
-                dd[k] = pd;
+                dd[k] = 1.0 / pd;
             } else {
                 dd[k] = 1.0;
             }
@@ -1345,7 +1345,7 @@ __global__ void __launch_bounds__(512, 1) k_pcg64d(PcgDev D, CoarseDev C)
 #pragma unroll
         for (int u = 0; u < 4; ++u) {
             const int k = k0 + u * NT;
-            if (k < nh) { dzh[k] = a[u]; vh[k] = isfinite(a[u]) ? c[u] / a[u] + ec[hown[k]] : 0.0; }
+            if (k < nh) { dzh[k] = a[u]; vh[k] = a[u] != 0.0 ? fma(c[u], a[u], ec[hown[k]]) : 0.0; }
         }
     }
     __syncthreads();
@@ -1355,7 +1355,7 @@ __global__ void __launch_bounds__(512, 1) k_pcg64d(PcgDev D, CoarseDev C)
     for (int k = 0; k < RMAX; ++k) {
         const int i = row_of(k);
         if (i < 0) continue;
-        const double zi = fr[k] ? r[k] / dd[k] + ec[s_own] : 0.0;
+        const double zi = fr[k] ? fma(r[k], dd[k], ec[s_own]) : 0.0;
         w[k] = fr[k] ? fma(D.pdiag[i], zi, off[k]) : 0.0;
         wb[0][i] = w[k];
         if (fr[k]) {
@@ -1410,7 +1410,7 @@ __global__ void __launch_bounds__(512, 1) k_pcg64d(PcgDev D, CoarseDev C)
                     if (k < nh) {
                         const double sj = fma(beta, a[u], c[u]);
                         const double rj = fma(-alpha, sj, e[u]);
-                        vh[k] = isfinite(dzh[k]) ? rj / dzh[k] + ec[hown[k]] : 0.0;
+                        vh[k] = dzh[k] != 0.0 ? fma(rj, dzh[k], ec[hown[k]]) : 0.0;
                     }
                 }
             }
@@ -1421,7 +1421,7 @@ __global__ void __launch_bounds__(512, 1) k_pcg64d(PcgDev D, CoarseDev C)
         for (int k = 0; k < RMAX; ++k) {
             const int i = row_of(k);
             if (i < 0) continue;
-            const double zo = r[k] / dd[k] + s_ecp;
+            const double zo = fma(r[k], dd[k], s_ecp);
             p[k] = fr[k] ? fma(beta, p[k], zo) : 0.0;
             s[k] = fma(beta, s[k], w[k]);
             if (fr[k]) D.pres[i] = fma(alpha, p[k], D.pres[i]);
@@ -1435,7 +1435,7 @@ __global__ void __launch_bounds__(512, 1) k_pcg64d(PcgDev D, CoarseDev C)
         for (int k = 0; k < RMAX; ++k) {
             const int i = row_of(k);
             if (i < 0) continue;
-            const double zi = fr[k] ? r[k] / dd[k] + ec[s_own] : 0.0;
+            const double zi = fr[k] ? fma(r[k], dd[k], ec[s_own]) : 0.0;
             w[k] = fr[k] ? fma(D.pdiag[i], zi, off[k]) : 0.0;
             wb[pn][i] = w[k];
             if (fr[k]) {
@@ -1536,7 +1536,7 @@ __global__ void __launch_bounds__(NT, NT >= 512 ? 1 : 2) k_pcg32m(PcgDev D)
             wmax = wr[k] > wmax ? wr[k] : wmax;
         }
         r[k] = p[k] = sv[k] = w[k] = 0.0f;
-        dd[k] = __int_as_float(0x7f800000);
+        dd[k] = 0.0f;   // reciprocal of the Jacobi diagonal; 0 off the free rows
         fr[k] = false;
     }
     // FP64 off-diagonal sums from the streamed FP64 coefficients and vh64
@@ -1627,7 +1627,7 @@ __global__ void __launch_bounds__(NT, NT >= 512 ? 1 : 2) k_pcg32m(PcgDev D)
 #pragma unroll
             for (int u = 0; u < 4; ++u) {
                 const int k = k0 + u * NT;
-                if (k < nh) { vz[k] = a[u] / dzh[k]; vp[k] = c[u]; }
+                if (k < nh) { vz[k] = a[u] * dzh[k]; vp[k] = c[u]; }
             }
         }
         __syncthreads();
@@ -1640,7 +1640,7 @@ __global__ void __launch_bounds__(NT, NT >= 512 ? 1 : 2) k_pcg32m(PcgDev D)
             if (i < 0) continue;
             if (zero_p) p[k] = 0.0f;
             const float pd = (float)D.pdiag[i];
-            const float zi = r[k] / dd[k];
+            const float zi = r[k] * dd[k];
             w[k] = fr[k] ? fmaf(pd, zi, offz[k]) : 0.0f;
             sv[k] = fr[k] ? fmaf(pd, p[k], offp[k]) : 0.0f;
             wb[buf][i] = w[k];
@@ -1667,7 +1667,7 @@ __global__ void __launch_bounds__(NT, NT >= 512 ? 1 : 2) k_pcg32m(PcgDev D)
         const double pd = D.pdiag[i];
         if (fr[k]) {
             if (g.precond && !(isfinite(pd) && pd > 1.0e-30)) acc.flag = fmax(acc.flag, 1.0);
-            dd[k] = g.precond ? (float)pd : 1.0f;
+            dd[k] = g.precond ? (float)(1.0 / pd) : 1.0f;
         }
         dz[i] = dd[k];
         sb[0][i] = 0.0f;
@@ -1722,7 +1722,7 @@ __global__ void __launch_bounds__(NT, NT >= 512 ? 1 : 2) k_pcg32m(PcgDev D)
                     if (k < nh) {
                         const float sj = fmaf(b32, a[u], c[u]);
                         const float rj = fmaf(-a32, sj, e[u]);
-                        vz[k] = rj / dzh[k];
+                        vz[k] = rj * dzh[k];
                     }
                 }
             }
@@ -1732,7 +1732,7 @@ __global__ void __launch_bounds__(NT, NT >= 512 ? 1 : 2) k_pcg32m(PcgDev D)
         for (int k = 0; k < RMAX; ++k) {
             const int i = row[k];
             if (i < 0) continue;
-            const float zo = r[k] / dd[k];
+            const float zo = r[k] * dd[k];
             p[k] = fr[k] ? fmaf(b32, p[k], zo) : 0.0f;
             sv[k] = fmaf(b32, sv[k], w[k]);
             if (fr[k]) D.pres[i] = fma(alpha, (double)p[k], D.pres[i]);
@@ -1747,7 +1747,7 @@ __global__ void __launch_bounds__(NT, NT >= 512 ? 1 : 2) k_pcg32m(PcgDev D)
         for (int k = 0; k < RMAX; ++k) {
             const int i = row[k];
             if (i < 0) continue;
-            const float zi = r[k] / dd[k];
+            const float zi = r[k] * dd[k];
             w[k] = fr[k] ? fmaf((float)D.pdiag[i], zi, off[k]) : 0.0f;
             wb[pn][i] = w[k];
             if (fr[k]) {
