@@ -193,6 +193,8 @@ def lib():
         L.cbs3d_batch_last_error.restype = cp
         L.cbs3d_selftest_wait_timeout.argtypes = [_i, ctypes.POINTER(_i)]
         L.cbs3d_selftest_wait_timeout.restype = _i
+        L.cbs3d_coarse_inverse.argtypes = [_i, _i, vp, vp, _i]
+        L.cbs3d_coarse_inverse.restype = _i
         for fn in ("cbs3d_create", "cbs3d_create_from_case", "cbs3d_read_params", "cbs3d_step",
                    "cbs3d_upload_fields", "cbs3d_download_fields", "cbs3d_get_array", "cbs3d_set_array",
                    "cbs3d_run_stage", "cbs3d_pressure_multiply", "cbs3d_pcg_create", "cbs3d_pcg_solve",
@@ -435,6 +437,19 @@ def selftest_wait_timeout(device: int = 0) -> int:
     if rc != 0:
         raise CBSError(rc, "selftest launch failed")
     return obs.value
+
+
+def coarse_inverse(a, variant: int = 0, device: int = 0) -> np.ndarray:
+    """Inverse of a small dense SPD matrix by the two-level preconditioner's
+    device Gauss-Jordan kernel (variant 0: register tiles, 1: shared memory)."""
+    a = np.ascontiguousarray(a, dtype=np.float64)
+    if a.ndim != 2 or a.shape[0] != a.shape[1]:
+        raise ValueError("square matrix expected")
+    out = np.empty_like(a)
+    rc = lib().cbs3d_coarse_inverse(device, a.shape[0], _ptr(a), _ptr(out), variant)
+    if rc != 0:
+        raise CBSError(rc, "coarse inverse failed")
+    return out
 
 
 class PressureSolver:

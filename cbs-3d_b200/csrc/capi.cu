@@ -950,6 +950,17 @@ cbs3d_status cbs3d_pcg_solve(cbs3d_pcg* p, int cg_preconditioner, int cg_conv_te
 
 void cbs3d_pcg_destroy(cbs3d_pcg* p) { delete p; }
 
+cbs3d_status cbs3d_coarse_inverse(int device, int g, const double* a, double* ainv, int variant)
+{
+    try {
+        return coarse_inverse(device, g, a, ainv, variant);
+    } catch (const Error& e) {
+        return e.code;
+    } catch (const std::exception&) {
+        return CBS3D_INTERNAL;
+    }
+}
+
 cbs3d_status cbs3d_selftest_wait_timeout(int device, int* observed_status)
 {
     try {

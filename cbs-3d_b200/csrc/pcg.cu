@@ -1869,6 +1869,84 @@ __global__ void __launch_bounds__(512) k_coarse_invert(int G, double* ac)
     for (int t = threadIdx.x; t < G * G; t += blockDim.x) ac[t] = a[t];
 }
 
+// The same Gauss-Jordan inverse with the matrix held in registers: thread
+// (ty = warp, tx = lane) of 16 x 32 owns rows ty + 16a (a < 10) and columns
+// tx + 32b (b < 5), so G <= 160.  Step k reads the old pivot row and column
+// from shared memory; the owners of row and column k+1 publish their new
+// values into the other half of a double buffer, so one barrier per pivot
+// suffices.  Every entry goes through the operations of k_coarse_invert in
+// the same order, so both give the same bits.
+constexpr int CINV_RA = 10, CINV_CB = 5, CINV_MAX = 160;
+__global__ void __launch_bounds__(512, 1) k_coarse_invert_reg(int G, double* ac)
+{
+    __shared__ double srow[2][CINV_MAX], scol[2][CINV_MAX];
+    const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
+    double v[CINV_RA][CINV_CB];
+#pragma unroll
+    for (int a = 0; a < CINV_RA; ++a)
+#pragma unroll
+        for (int b = 0; b < CINV_CB; ++b) {
+            const int i = ty + 16 * a, j = tx + 32 * b;
+            double x = (i < G && j < G) ? ac[(size_t)i * G + j] : 0.0;
+            if (i == j && i < G && x == 0.0) x = 1.0;
+            v[a][b] = x;
+        }
+    for (int t = threadIdx.x; t < 2 * CINV_MAX; t += blockDim.x) {
+        (&srow[0][0])[t] = 0.0;
+        (&scol[0][0])[t] = 0.0;
+    }
+    __syncthreads();
+    if (ty == 0)
+#pragma unroll
+        for (int b = 0; b < CINV_CB; ++b) srow[0][tx + 32 * b] = v[0][b];
+    if (tx == 0)
+#pragma unroll
+        for (int a = 0; a < CINV_RA; ++a) scol[0][ty + 16 * a] = v[a][0];
+    for (int k = 0; k < G; ++k) {
+        __syncthreads();
+        const int cur = k & 1, nxt = cur ^ 1;
+        const double pinv = 1.0 / srow[cur][k];
+        double rk[CINV_CB];
+#pragma unroll
+        for (int b = 0; b < CINV_CB; ++b) rk[b] = srow[cur][tx + 32 * b] * pinv;
+        // elimination, with column k and row k selected in place
+#pragma unroll
+        for (int a = 0; a < CINV_RA; ++a) {
+            const int i = ty + 16 * a;
+            const double ci = scol[cur][i];
+            const double cneg = -ci * pinv;
+#pragma unroll
+            for (int b = 0; b < CINV_CB; ++b) {
+                const int j = tx + 32 * b;
+                const double t = fma(-ci, rk[b], v[a][b]);
+                v[a][b] = (i == k) ? ((j == k) ? pinv : rk[b]) : ((j == k) ? cneg : t);
+            }
+        }
+        const int k1 = k + 1;
+        if (k1 < G) {
+            if ((k1 & 15) == ty)
+#pragma unroll
+                for (int a = 0; a < CINV_RA; ++a)
+                    if (ty + 16 * a == k1)
+#pragma unroll
+                        for (int b = 0; b < CINV_CB; ++b) srow[nxt][tx + 32 * b] = v[a][b];
+            if ((k1 & 31) == tx)
+#pragma unroll
+                for (int b = 0; b < CINV_CB; ++b)
+                    if (tx + 32 * b == k1)
+#pragma unroll
+                        for (int a = 0; a < CINV_RA; ++a) scol[nxt][ty + 16 * a] = v[a][b];
+        }
+    }
+#pragma unroll
+    for (int a = 0; a < CINV_RA; ++a)
+#pragma unroll
+        for (int b = 0; b < CINV_CB; ++b) {
+            const int i = ty + 16 * a, j = tx + 32 * b;
+            if (i < G && j < G) ac[(size_t)i * G + j] = v[a][b];
+        }
+}
+
 // Self-test of the bounded device wait: CTA 0 leaves without arriving, so the
 // other CTAs' barrier waits can only end by running out of their spin limit.
 __global__ void k_barrier_selftest(unsigned* bar, DevStatus* st)
@@ -1894,6 +1972,30 @@ cbs3d_status selftest_wait_timeout(int device, int* observed)
     cudaFree(bar);
     cudaFree(st);
     if (observed) *observed = h.code;
+    return CBS3D_OK;
+}
+
+cbs3d_status coarse_inverse(int device, int g, const double* a, double* ainv, int variant)
+{
+    if (!a || !ainv || g < 1 || (variant != 0 && variant != 1) || g > (variant == 0 ? CINV_MAX : 164))
+        return CBS3D_INVALID_INPUT;
+    CUDA_OK(cudaSetDevice(device));
+    const size_t bytes = static_cast<size_t>(g) * g * sizeof(double);
+    double* d = dalloc<double>(static_cast<size_t>(g) * g);
+    cudaError_t e = cudaMemcpy(d, a, bytes, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) {
+        if (variant == 0) {
+            k_coarse_invert_reg<<<1, 512>>>(g, d);
+        } else {
+            const size_t ismem = (static_cast<size_t>(g) * g + 2 * static_cast<size_t>(g)) * 8;
+            e = raise_smem_limit(reinterpret_cast<const void*>(k_coarse_invert), ismem);
+            if (e == cudaSuccess) k_coarse_invert<<<1, 512, ismem>>>(g, d);
+        }
+        if (e == cudaSuccess) e = cudaGetLastError();
+        if (e == cudaSuccess) e = cudaMemcpy(ainv, d, bytes, cudaMemcpyDeviceToHost);
+    }
+    cudaFree(d);
+    CUDA_OK(e);
     return CBS3D_OK;
 }
 
@@ -2282,7 +2384,10 @@ cbs3d_status PcgEngine::solve(double* pres, double* rhs1, double* pdiag, int pre
         CUDA_OK(cudaMemsetAsync(d_ac, 0, static_cast<size_t>(G) * G * sizeof(double), st));
         k_coarse_blocks<<<static_cast<unsigned>(npairs), 256, 0, st>>>(d_pair_ptr, d_pair_ij, d_pair_ent, d_val, d_dp, G,
                                                                       d_ac);
-        k_coarse_invert<<<1, 512, coarse_ismem, st>>>(G, d_ac);
+        if (G <= CINV_MAX)
+            k_coarse_invert_reg<<<1, 512, 0, st>>>(G, d_ac);
+        else
+            k_coarse_invert<<<1, 512, coarse_ismem, st>>>(G, d_ac);
         fn = fn_twolevel(rmax);
         smem = coarse_smem;
     }

@@ -233,4 +233,8 @@ private:
 // the bounded waits recorded (CBS3D_TIMEOUT when they ran out as designed).
 cbs3d_status selftest_wait_timeout(int device, int* observed);
 
+// Inverts a g x g host matrix with the coarse-operator Gauss-Jordan kernels
+// (variant 0: registers, g <= 160; 1: shared memory, g <= 164).
+cbs3d_status coarse_inverse(int device, int g, const double* a, double* ainv, int variant);
+
 }  // namespace cbs3d

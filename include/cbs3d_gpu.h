@@ -360,6 +360,15 @@ const char* cbs3d_batch_last_error(const cbs3d_batch* b);
  * CBS3D_TIMEOUT after about a second.  The device stays usable. */
 cbs3d_status cbs3d_selftest_wait_timeout(int device, int* observed_status);
 
+/* Dense inverse of a g x g row-major matrix by the device Gauss-Jordan
+ * kernels that invert the two-level preconditioner's aggregated operator
+ * (no reference counterpart; the coarse space is an extension).  variant 0:
+ * the register-tiled kernel (g <= 160, the one solves use); 1: the
+ * shared-memory kernel (g <= 164).  No pivoting: meant for SPD matrices; a
+ * zero diagonal entry is replaced by 1 first, as for an empty aggregate.
+ * a and ainv are host arrays of g*g doubles. */
+cbs3d_status cbs3d_coarse_inverse(int device, int g, const double* a, double* ainv, int variant);
+
 #ifdef __cplusplus
 }
 #endif

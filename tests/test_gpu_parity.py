@@ -260,3 +260,26 @@ def test_two_level_matches_jacobi():
     (ua, pa, _), (ub, pb, _) = a.fields(), b.fields()
     assert rel_l2(ub, ua) <= RUN_TOL
     assert rel_l2(pb, pa) <= RUN_TOL
+
+
+@pytest.mark.parametrize("g", [1, 37, 148, 160])
+def test_coarse_inverse_kernels(g):
+    """The two device Gauss-Jordan kernels for the two-level preconditioner's
+    aggregated operator (register tiles, the one solves use; shared memory)
+    give the same bits, match numpy's inverse of a seeded SPD matrix to 1e-12,
+    and treat an empty aggregate (zero row, column and diagonal) as identity."""
+    gpu = _gpu()
+    rng = np.random.default_rng(7 + g)
+    b = rng.standard_normal((g, g))
+    a = b @ b.T / g + np.diag(rng.uniform(0.5, 2.0, g))
+    if g > 2:
+        a[g // 2, :] = 0.0
+        a[:, g // 2] = 0.0
+    r = gpu.coarse_inverse(a, variant=0)
+    s = gpu.coarse_inverse(a, variant=1)
+    assert bitwise(r, s)
+    a1 = a.copy()
+    if g > 2:
+        a1[g // 2, g // 2] = 1.0
+    ref = np.linalg.inv(a1)
+    assert np.linalg.norm(r - ref) / np.linalg.norm(ref) <= 1e-12

@@ -182,3 +182,11 @@ def test_abi_rejects_bad_inputs_before_touching_a_device():
     assert L.cbs3d_pcg_create(c.mesh.nelem, c.mesh.npoin, gpu._ptr(good), None, 1, gpu._ptr(bl), gpu._ptr(bv), None,
                               ctypes.byref(pcg), err, 512) == 1
     assert b"fixed pressure node out of range" in err.value
+    # the coarse-operator inverse checks its size and variant before any device call
+    m = np.eye(3)
+    out = np.empty_like(m)
+    assert L.cbs3d_coarse_inverse(0, 0, gpu._ptr(m), gpu._ptr(out), 0) == 1
+    assert L.cbs3d_coarse_inverse(0, 161, gpu._ptr(m), gpu._ptr(out), 0) == 1
+    assert L.cbs3d_coarse_inverse(0, 165, gpu._ptr(m), gpu._ptr(out), 1) == 1
+    assert L.cbs3d_coarse_inverse(0, 3, gpu._ptr(m), gpu._ptr(out), 2) == 1
+    assert L.cbs3d_coarse_inverse(0, 3, None, gpu._ptr(out), 0) == 1
