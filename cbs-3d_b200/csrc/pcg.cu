@@ -728,7 +728,8 @@ struct Acc6 {
 // phase parity), arrives on a 64-bit counter that only grows, waits until
 // all G CTAs of this phase have arrived, and then reduces the G partials
 // itself in a fixed order (thread t takes CTAs t, t+T, ...; warp shuffles;
-// warps in order).  Every CTA therefore computes bit-identical totals without
+// warps in order).  The partials are stored value-major (value q of CTA b at
+// q*G + b), so a warp reading one value of 32 CTAs touches two L2 lines.  Every CTA therefore computes bit-identical totals without
 // a second round trip through a last-arriving CTA.  The caller passes the
 // number of all-reduces this launch has completed as `phase`.  Returns false
 // when the wait gave up (status TIMEOUT) or another CTA raised a status.
@@ -762,9 +763,8 @@ __device__ __forceinline__ bool grid_allreduce_v(double (&v)[NV], const PcgDev& 
         for (int k = 0; k < (NT / 32); ++k)
 #pragma unroll
             for (int q = 0; q < NV; ++q) t[q] = q < NSUM ? t[q] + sm[k][q] : fmax(t[q], sm[k][q]);
-        double* p = part + (size_t)g.b * 8;
 #pragma unroll
-        for (int q = 0; q < NV; ++q) __stcg(p + q, t[q]);
+        for (int q = 0; q < NV; ++q) __stcg(part + (q * G + g.b), t[q]);
         const unsigned long long target = (unsigned long long)(phase + 1) * (unsigned long long)G;
         unsigned long long arrived;
         asm volatile("atom.add.acq_rel.gpu.global.u64 %0, [%1], 1;" : "=l"(arrived) : "l"(cnt) : "memory");
@@ -793,9 +793,11 @@ __device__ __forceinline__ bool grid_allreduce_v(double (&v)[NV], const PcgDev& 
     for (int q = 0; q < NV; ++q) t[q] = 0.0;
     if (ok) {
         for (int k = threadIdx.x; k < G; k += NT) {
-            const double* p = part + (size_t)k * 8;
 #pragma unroll
-            for (int q = 0; q < NV; ++q) t[q] = q < NSUM ? t[q] + __ldcg(p + q) : fmax(t[q], __ldcg(p + q));
+            for (int q = 0; q < NV; ++q) {
+                const double x = __ldcg(part + (q * G + k));
+                t[q] = q < NSUM ? t[q] + x : fmax(t[q], x);
+            }
         }
     }
 #pragma unroll
@@ -874,10 +876,8 @@ __device__ __forceinline__ bool grid_allreduce3g(Acc6 v, double x, const PcgDev&
         for (int k = 0; k < NW; ++k)
 #pragma unroll
             for (int q = 0; q < 6; ++q) t[q] = (q < 3 || q == 5) ? t[q] + sm[k][q] : fmax(t[q], sm[k][q]);
-        double* p = part + (size_t)g.b * 8;
 #pragma unroll
-        for (int q = 0; q < 5; ++q) __stcg(p + q, t[q]);
-        __stcg(p + 7, t[5]);
+        for (int q = 0; q < 6; ++q) __stcg(part + (q * G + g.b), t[q]);
         const unsigned long long target = (unsigned long long)(phase + 1) * (unsigned long long)G;
         unsigned long long arrived;
         asm volatile("atom.add.acq_rel.gpu.global.u64 %0, [%1], 1;" : "=l"(arrived) : "l"(cnt) : "memory");
@@ -904,10 +904,12 @@ __device__ __forceinline__ bool grid_allreduce3g(Acc6 v, double x, const PcgDev&
     double t[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
     if (ok) {
         for (int k = threadIdx.x; k < G; k += NT) {
-            const double* p = part + (size_t)k * 8;
 #pragma unroll
-            for (int q = 0; q < 5; ++q) t[q] = q < 3 ? t[q] + __ldcg(p + q) : fmax(t[q], __ldcg(p + q));
-            cvec[k] = __ldcg(p + 7);
+            for (int q = 0; q < 5; ++q) {
+                const double y = __ldcg(part + (q * G + k));
+                t[q] = q < 3 ? t[q] + y : fmax(t[q], y);
+            }
+            cvec[k] = __ldcg(part + (5 * G + k));
         }
     }
 #pragma unroll
