@@ -167,6 +167,10 @@ def lib():
         L.cbs3d_write_vtu_case.restype = _i
         L.cbs3d_write_vtu.argtypes = [vp, cp]
         L.cbs3d_write_vtu.restype = _i
+        L.cbs3d_write_vtu_async.argtypes = [vp, cp]
+        L.cbs3d_write_vtu_async.restype = _i
+        L.cbs3d_vtu_flush.argtypes = [vp]
+        L.cbs3d_vtu_flush.restype = _i
         L.cbs3d_write_residual_rows.argtypes = [vp, cp, _i]
         L.cbs3d_write_residual_rows.restype = _i
         L.cbs3d_step_history.argtypes = [vp, _i, _i, vp]
@@ -310,6 +314,18 @@ class Context:
     def _check(self, rc: int):
         if rc != 0:
             raise CBSError(rc, lib().cbs3d_last_error(self.h).decode())
+
+    def write_vtu(self, path: str):
+        """VTU snapshot of the current fields (Post::writeVTU), written now."""
+        self._check(lib().cbs3d_write_vtu(self.h, path.encode()))
+
+    def write_vtu_async(self, path: str):
+        """The same snapshot, taken on the device and written by a host
+        thread while later steps run; vtu_flush() waits for the files."""
+        self._check(lib().cbs3d_write_vtu_async(self.h, path.encode()))
+
+    def vtu_flush(self):
+        self._check(lib().cbs3d_vtu_flush(self.h))
 
     def _get_len(self, name: str) -> int:
         n = ctypes.c_long(0)

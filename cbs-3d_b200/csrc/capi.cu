@@ -1337,6 +1337,26 @@ cbs3d_status cbs3d_write_vtu(cbs3d_ctx* c, const char* path)
     });
 }
 
+cbs3d_status cbs3d_write_vtu_async(cbs3d_ctx* c, const char* path)
+{
+    return guarded(c, [&] {
+        if (!path) throw Error(CBS3D_INVALID_INPUT, "cbs3d_write_vtu_async - path required");
+        CUDA_OK(cudaSetDevice(c->opt.device));
+        if (!c->snaps) c->snaps.reset(new VtuSnapshots(c->opt.device, c->m, c->m.N));
+        // before the first step the device magnitude is not yet computed
+        c->snaps->enqueue(c->st, c->S.unkno, c->S.pres, c->S.temp, c->iitime > 0 ? c->S.velocity : nullptr, path);
+    });
+}
+
+cbs3d_status cbs3d_vtu_flush(cbs3d_ctx* c)
+{
+    return guarded(c, [&] {
+        if (!c->snaps) return;
+        const std::string e = c->snaps->flush();
+        if (!e.empty()) throw Error(CBS3D_IO_ERROR, e);
+    });
+}
+
 cbs3d_status cbs3d_write_vtu_case(const char* case_name, const char* path, const double* u, const double* p,
                                   const double* t, char* err, size_t errlen)
 {

@@ -7,7 +7,9 @@
 #include "host_model.h"
 #include "kernels.cuh"
 #include "pcg.cuh"
+#include "snapshot.cuh"
 
+#include <memory>
 #include <string>
 #include <vector>
 
@@ -80,8 +82,11 @@ struct cbs3d_ctx {
     double* d_bforce = nullptr;        // body force f[3N] (extension), when set
     double* d_mfluid = nullptr;        // fluid lumped mass, for the body force
 
+    std::unique_ptr<VtuSnapshots> snaps;   // asynchronous VTU writer, made on first use
+
     ~cbs3d_ctx()
     {
+        snaps.reset();   // pending snapshots are written before the fields go away
         for (cudaEvent_t e : pcg_ev) cudaEventDestroy(e);
         if (gexec) cudaGraphExecDestroy(gexec);
         pcg.release();

@@ -72,7 +72,8 @@ int main(int argc, char** argv)
         double rtime = 0.0;
         auto write_solution = [&](int it) {
             const std::string f = name + "_" + step_tag(it) + ".vtu";
-            check(cbs3d_write_vtu(ctx, (outdir / f).string().c_str()), ctx, "writeVTU");
+            // taken on the device now, written by the context's writer thread
+            check(cbs3d_write_vtu_async(ctx, (outdir / f).string().c_str()), ctx, "writeVTU");
             vtus.push_back(f);
             times.push_back(rtime);
             std::vector<const char*> fp;
@@ -114,6 +115,7 @@ int main(int argc, char** argv)
             }
         }
         if (vtu && (vtus.empty() || vtus.back() != name + "_" + step_tag(last) + ".vtu")) write_solution(last);
+        check(cbs3d_vtu_flush(ctx), ctx, "writeVTU");
         const double wall = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
         std::printf("%s: %d steps (%s); last PCG %d iterations, rel %.3e; %.3f s on the device, %.3f s total\n",
                     name.c_str(), last, reason.c_str(), st.cg.iterations, st.cg.final_relative_l2, gpu_seconds, wall);

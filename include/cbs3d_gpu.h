@@ -229,6 +229,19 @@ cbs3d_status cbs3d_step_history(cbs3d_ctx* ctx, int first, int count, double* re
  * header != 0), honouring residual_log_enabled / residual_log_every. */
 cbs3d_status cbs3d_write_residual_rows(cbs3d_ctx* ctx, const char* path, int header);
 cbs3d_status cbs3d_write_vtu(cbs3d_ctx* ctx, const char* path);
+/* The same file written off the step path: the fields are copied on the
+ * device on the context's stream (microseconds), copied to pinned host
+ * memory on a side stream and written by a host thread of the context, so
+ * the call returns at once and later steps overlap the copy-out and the
+ * file write.  The file holds the fields as they are when the work already
+ * issued on the context has run.  Two snapshots may be in flight; a third
+ * call waits for the oldest to be written.  The first call allocates the
+ * two snapshot slots (6 doubles per node each, device and pinned host).
+ * cbs3d_vtu_flush waits for every pending file and returns the first write
+ * error since the previous flush (CBS3D_IO_ERROR); cbs3d_destroy writes
+ * what is pending.  No reference counterpart for the asynchrony. */
+cbs3d_status cbs3d_write_vtu_async(cbs3d_ctx* ctx, const char* path);
+cbs3d_status cbs3d_vtu_flush(cbs3d_ctx* ctx);
 /* Host only: the VTU of a case's mesh with caller fields (u[3N], p[N], t[N]). */
 cbs3d_status cbs3d_write_vtu_case(const char* case_name, const char* path, const double* u, const double* p,
                                   const double* t, char* err, size_t errlen);

@@ -61,3 +61,33 @@ def test_driver_reports_reference_errors(tmp_path):
     r = subprocess.run([DRIVER, base], cwd=str(tmp_path), capture_output=True, text=True, timeout=120)
     assert r.returncode == 1
     assert "unsupported solver BC ID 777" in r.stderr
+
+
+def test_async_vtu_matches_immediate_vtu(tmp_path):
+    """cbs3d_write_vtu_async gives the same file as cbs3d_write_vtu taken at
+    the same point, although later steps are issued before it is written;
+    three snapshots in a row exercise the wait for a free slot, and flush
+    reports a file that cannot be written."""
+    from cbs3d import gpu
+    case, _ = load_case(fixture_path("cav6j"))
+    ctx = gpu.Context(case)
+    ctx.write_vtu(str(tmp_path / "s0.vtu"))
+    ctx.write_vtu_async(str(tmp_path / "a0.vtu"))
+    pairs = [("s0.vtu", "a0.vtu")]
+    for k in (1, 2, 3):
+        ctx.step(k)
+        ctx.write_vtu(str(tmp_path / f"s{k}.vtu"))
+        ctx.write_vtu_async(str(tmp_path / f"a{k}.vtu"))
+        pairs.append((f"s{k}.vtu", f"a{k}.vtu"))
+    ctx.step(2)   # issued while the last snapshots may still be copied out
+    ctx.vtu_flush()
+    for s, a in pairs:
+        assert (tmp_path / s).read_bytes() == (tmp_path / a).read_bytes(), (s, a)
+    ctx.write_vtu_async(str(tmp_path / "no_such_dir" / "x.vtu"))
+    with pytest.raises(gpu.CBSError) as e:
+        ctx.vtu_flush()
+    assert e.value.code == 7 and "x.vtu" in e.value.message
+    ctx.vtu_flush()   # the error is reported once
+    ctx.write_vtu_async(str(tmp_path / "last.vtu"))
+    ctx.close()       # writes what is pending
+    assert (tmp_path / "last.vtu").stat().st_size > 0
