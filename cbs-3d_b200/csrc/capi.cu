@@ -98,6 +98,10 @@ void cbs3d_ctx::setup(bool own_pcg)
     CUDA_OK(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
     CUDA_OK(cudaEventCreate(&ev0));
     CUDA_OK(cudaEventCreate(&ev1));
+    CUDA_OK(cudaStreamCreateWithFlags(&side, cudaStreamNonBlocking));
+    CUDA_OK(cudaEventCreateWithFlags(&ev_fork, cudaEventDisableTiming));
+    CUDA_OK(cudaEventCreateWithFlags(&ev_join, cudaEventDisableTiming));
+    own_engine = own_pcg;
     const size_t E = m.E, N = m.N;
     DevParams& P = S.P;
     P.E = m.E; P.N = m.N; P.NB = m.NB;
@@ -219,9 +223,28 @@ void cbs3d_ctx::stage_time_step(int it)
     if (!fx && force_global()) k_dt_force<<<nb(m.E), T, 0, st>>>(S);
 }
 
+// The pressure operator depends on delte and the LHS only, so once the last
+// LHS update of a step is issued it is assembled (with the two-level set-up)
+// on the side stream while Steps 1 and 2 run; stage_solve joins it.
+void cbs3d_ctx::fork_assembly()
+{
+    if (!own_engine) return;
+    CUDA_OK(cudaEventRecord(ev_fork, st));
+    CUDA_OK(cudaStreamWaitEvent(side, ev_fork, 0));
+    pcg.assemble_from_state(S, side);
+    pcg.prepare_coarse(S.pdiag, side);
+    CUDA_OK(cudaEventRecord(ev_join, side));
+    assembly_forked = true;
+}
+
 void cbs3d_ctx::stage_solve()
 {
-    pcg.assemble_from_state(S, st);
+    if (assembly_forked) {
+        CUDA_OK(cudaStreamWaitEvent(st, ev_join, 0));
+        assembly_forked = false;
+    } else {
+        pcg.assemble_from_state(S, st);
+    }
     cudaEvent_t e0 = nullptr, e1 = nullptr;
     if (opt.time_pcg) {
         while (static_cast<int>(pcg_ev.size()) < pcg_ev_used + 2) {
@@ -242,11 +265,13 @@ void cbs3d_ctx::enqueue_pre(int it)
     k_begin_step<<<nb(m.N), T, 0, st>>>(S);
     stage_time_step(it);
     k_lhs<<<nb(m.N), T, 0, st>>>(S);
+    if (m.p.step2_check <= 0) fork_assembly();
     k_step1_elem<<<nb(m.E, 128), 128, 0, st>>>(S);
     k_step1_node<<<nb(m.N), T, 0, st>>>(S);
     if (m.p.step2_check > 0) {
         k_dt_correction<<<nb(m.E), T, 0, st>>>(S);
         k_lhs<<<nb(m.N), T, 0, st>>>(S);
+        fork_assembly();
     }
     k_step2_elem<<<nb(m.E), T, 0, st>>>(S);
     k_step2_node<<<nb(m.N), T, 0, st>>>(S);

@@ -71,6 +71,11 @@ struct cbs3d_ctx {
     long long cg_total = 0;
     std::string err;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    // operator assembly (and two-level set-up) of the pressure solve, forked
+    // onto `side` after the last LHS update so that it overlaps Steps 1-2
+    cudaStream_t side = nullptr;
+    cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
+    bool own_engine = false, assembly_forked = false;
     cudaGraphExec_t gexec = nullptr;
     bool graph_failed = false;
     std::vector<cudaEvent_t> pcg_ev;   // 2 per step when timing PCG launches
@@ -93,6 +98,9 @@ struct cbs3d_ctx {
         buf.release();
         if (ev0) cudaEventDestroy(ev0);
         if (ev1) cudaEventDestroy(ev1);
+        if (ev_fork) cudaEventDestroy(ev_fork);
+        if (ev_join) cudaEventDestroy(ev_join);
+        if (side) cudaStreamDestroy(side);
         if (st) cudaStreamDestroy(st);
     }
 
@@ -113,6 +121,7 @@ struct cbs3d_ctx {
     void reset_status() { CUDA_OK(cudaMemsetAsync(S.status, 0, sizeof(DevStatus), st)); }
     void stage_time_step(int it);
     void stage_solve();
+    void fork_assembly();
     // Solver::advanceOneStep in two halves around the pressure solve
     void enqueue_pre(int it);
     void enqueue_post(int it);

@@ -1815,15 +1815,18 @@ __global__ void __launch_bounds__(NT, NT >= 512 ? 1 : 2) k_pcg32m(PcgDev D)
 // Aggregated operator P^T A P of the free rows: one CTA per nonzero (I, J)
 // block; thread t sums entries t, t+T, ... (coefficient slots, or the
 // diagonal of row -e-1), then warps and the CTA reduce in a fixed order.
+// The diagonal is read by row position, or through row_node when that is
+// given (the node-ordered diagonal: the same values on free rows).
 __global__ void __launch_bounds__(256) k_coarse_blocks(const int* pair_ptr, const int2* pair_ij, const int* ent,
-                                                       const double* val, const double* pdiag_pos, int G, double* ac)
+                                                       const double* val, const double* pdiag, const int* row_node,
+                                                       int G, double* ac)
 {
     __shared__ double sm[8];
     const int q = blockIdx.x;
     double s = 0.0;
     for (int k = pair_ptr[q] + threadIdx.x; k < pair_ptr[q + 1]; k += 256) {
         const int e = ent[k];
-        s += e >= 0 ? val[e] : pdiag_pos[-e - 1];
+        s += e >= 0 ? val[e] : pdiag[row_node ? row_node[-e - 1] : -e - 1];
     }
     for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
     if ((threadIdx.x & 31) == 0) sm[threadIdx.x >> 5] = s;
@@ -2323,6 +2326,25 @@ void PcgEngine::release()
     d_xp = d_bp = d_dp = nullptr; d_fp = nullptr;
 }
 
+void PcgEngine::coarse_setup(const double* pdiag, const int* row_node, cudaStream_t st)
+{
+    const int G = nblocks;
+    CUDA_OK(cudaMemsetAsync(d_ac, 0, static_cast<size_t>(G) * G * sizeof(double), st));
+    k_coarse_blocks<<<static_cast<unsigned>(npairs), 256, 0, st>>>(d_pair_ptr, d_pair_ij, d_pair_ent, d_val, pdiag,
+                                                                  row_node, G, d_ac);
+    if (G <= CINV_MAX)
+        k_coarse_invert_reg<<<1, 512, 0, st>>>(G, d_ac);
+    else
+        k_coarse_invert<<<1, 512, coarse_ismem, st>>>(G, d_ac);
+}
+
+void PcgEngine::prepare_coarse(const double* d_pdiag_node, cudaStream_t st)
+{
+    if (!coarse) return;
+    coarse_setup(d_pdiag_node, d_row_node, st);
+    coarse_ready = true;
+}
+
 void PcgEngine::assemble_from_state(const DevState& S, cudaStream_t st)
 {
     if (!nslots) return;
@@ -2381,15 +2403,10 @@ cbs3d_status PcgEngine::solve(double* pres, double* rhs1, double* pdiag, int pre
     CoarseDev C = cdev;
     void* args2[] = {&D, &C};
     if (coarse) {
-        // the aggregated operator of this solve and its inverse
-        const int G = nblocks;
-        CUDA_OK(cudaMemsetAsync(d_ac, 0, static_cast<size_t>(G) * G * sizeof(double), st));
-        k_coarse_blocks<<<static_cast<unsigned>(npairs), 256, 0, st>>>(d_pair_ptr, d_pair_ij, d_pair_ent, d_val, d_dp, G,
-                                                                      d_ac);
-        if (G <= CINV_MAX)
-            k_coarse_invert_reg<<<1, 512, 0, st>>>(G, d_ac);
-        else
-            k_coarse_invert<<<1, 512, coarse_ismem, st>>>(G, d_ac);
+        // the aggregated operator of this solve and its inverse, unless
+        // prepare_coarse made them already
+        if (!coarse_ready) coarse_setup(d_dp, nullptr, st);
+        coarse_ready = false;
         fn = fn_twolevel(rmax);
         smem = coarse_smem;
     }

@@ -92,6 +92,10 @@ public:
     void release();
     // ELL values from gstifE*delte (step path) or from a caller's gstif[6E].
     void assemble_from_state(const DevState& S, cudaStream_t st);
+    // Two-level set-up of the next solve (aggregated operator and its
+    // inverse) from the assembled operator and the node-ordered diagonal,
+    // on `st`; that solve then skips its own set-up.  No-op without coarse.
+    void prepare_coarse(const double* d_pdiag_node, cudaStream_t st);
     void assemble_from_gstif(const double* d_gstif, cudaStream_t st);
     // Runs one solve on pres/rhs1/pdiag (device pointers), result to host.
     // ev0/ev1 (optional) are recorded around the persistent PCG launch.
@@ -108,6 +112,7 @@ public:
     int rmax = 0;            // rows per thread of the register-resident kernels (0: global kernel)
     int nthreads = 512;      // CTA size of the persistent kernel
     bool coarse = false;     // two-level preconditioner in use
+    bool coarse_ready = false;   // prepare_coarse ran for the next solve
     size_t coarse_smem = 0, coarse_ismem = 0;
     int npairs = 0, sms_ = 0;
     int *d_pair_ptr = nullptr, *d_pair_ent = nullptr, *d_nbr_ptr = nullptr, *d_nbr_ids = nullptr;
@@ -117,6 +122,7 @@ public:
     CoarseDev cdev{};
     std::vector<int> h_hptr, h_hidx;
     void build_coarse(const HostModel& m, const std::vector<int>& colp);
+    void coarse_setup(const double* pdiag, const int* row_node, cudaStream_t st);
     int variant = 1;         // 1 global vectors, 2 register rows, 3 + shared-memory halo, 4 + one sync per iteration
     size_t halo_smem = 0;    // dynamic shared memory of the halo kernel
     size_t mixed_smem = 0;   // dynamic shared memory of the mixed-precision kernel
