@@ -950,6 +950,12 @@ __global__ void __launch_bounds__(NT, NT >= 512 ? 1 : 2) k_pcg64c(PcgDev D)
     double* dzh = vh + D.halo_max;
     int* hidx = reinterpret_cast<int*>(dzh + D.halo_max);
     unsigned short* lcs = reinterpret_cast<unsigned short*>(hidx + D.halo_max);
+    // the own rows' pressure and diagonal, kept in shared memory for the
+    // solve when the engine sized it so (the two-CTAs-per-SM kernel of small
+    // meshes only; the other instantiations compile the global accesses alone)
+    constexpr bool XS = NT == 256 && !BATCH;
+    double* xs = XS && D.xs_off ? reinterpret_cast<double*>(smem_raw + D.xs_off) : nullptr;
+    double* pds = xs ? xs + RMAX * NT : nullptr;
     for (int k = threadIdx.x; k < nh; k += NT) hidx[k] = D.halo_idx[h0 + k];
     for (int k = threadIdx.x; k < nsl; k += NT) lcs[k] = D.lcol[S0 + k];
     int phase = 0;
@@ -1025,7 +1031,12 @@ __global__ void __launch_bounds__(NT, NT >= 512 ? 1 : 2) k_pcg64c(PcgDev D)
         const bool active = f & 1;
         fr[k] = (f & 1) && !(f & 4);
         const double pd = D.pdiag[i];
-        const double y = fma(pd, D.pres[i], off[k]);
+        const double xi = D.pres[i];
+        if (xs) {
+            xs[k * NT + threadIdx.x] = xi;
+            pds[k * NT + threadIdx.x] = pd;
+        }
+        const double y = fma(pd, xi, off[k]);
         double ri = active ? D.rhs1[i] - y : 0.0;
         if (!fr[k]) ri = 0.0;
         if (fr[k]) {
@@ -1044,6 +1055,13 @@ __global__ void __launch_bounds__(NT, NT >= 512 ? 1 : 2) k_pcg64c(PcgDev D)
         dz[i] = dd[k];
         sb[0][i] = 0.0;
     }
+    // the pressure of the free own rows back to global memory
+    auto store_x = [&]() {
+        if (!xs) return;
+#pragma unroll
+        for (int k = 0; k < RMAX; ++k)
+            if (row[k] >= 0 && fr[k]) D.pres[row[k]] = xs[k * NT + threadIdx.x];
+    };
     Acc6 t{0.0, 0.0, 0.0, 0.0, 0.0};
     if (!grid_allreduce3<NT>(acc, D, g, phase, t)) return;
     ++phase;
@@ -1078,7 +1096,7 @@ __global__ void __launch_bounds__(NT, NT >= 512 ? 1 : 2) k_pcg64c(PcgDev D)
         const int i = row[k];
         if (i < 0) continue;
         const double zi = r[k] * dd[k];
-        w[k] = fr[k] ? fma(D.pdiag[i], zi, off[k]) : 0.0;
+        w[k] = fr[k] ? fma(xs ? pds[k * NT + threadIdx.x] : D.pdiag[i], zi, off[k]) : 0.0;
         wb[0][i] = w[k];
         if (fr[k]) {
             acc.a = fma(r[k], zi, acc.a);
@@ -1086,7 +1104,7 @@ __global__ void __launch_bounds__(NT, NT >= 512 ? 1 : 2) k_pcg64c(PcgDev D)
         }
     }
     t = Acc6{0.0, 0.0, 0.0, 0.0, 0.0};
-    if (!grid_allreduce3<NT>(acc, D, g, phase, t)) return;
+    if (!grid_allreduce3<NT>(acc, D, g, phase, t)) { store_x(); return; }
     ++phase;
     double gam = t.a;
     if (gam <= 1.0e-300 || !isfinite(gam)) { if (b == 0 && threadIdx.x == 0) set_status(seg_status(D, g), 3, ST_PCG, 0, R_PCG_RZ0); return; }
@@ -1094,7 +1112,7 @@ __global__ void __launch_bounds__(NT, NT >= 512 ? 1 : 2) k_pcg64c(PcgDev D)
     double beta = 0.0, fin = init, rel = 1.0, mx = 0.0, alpha = 0.0;
     int it = 0, conv = 0;
     for (it = 1; it <= g.max_iter; ++it) {
-        if (fabs(den) <= 1.0e-300 || !isfinite(den)) { if (b == 0 && threadIdx.x == 0) set_status(seg_status(D, g), 3, ST_PCG, it, R_PCG_PAP); return; }
+        if (fabs(den) <= 1.0e-300 || !isfinite(den)) { store_x(); if (b == 0 && threadIdx.x == 0) set_status(seg_status(D, g), 3, ST_PCG, it, R_PCG_PAP); return; }
         alpha = gam / den;
         const int po = (it - 1) & 1, pn = it & 1;
         // stage z_it of the halo: s = w_o + beta*s_o, r = r_o - alpha*s, z = r / dz
@@ -1135,7 +1153,10 @@ __global__ void __launch_bounds__(NT, NT >= 512 ? 1 : 2) k_pcg64c(PcgDev D)
             const double zo = r[k] * dd[k];
             p[k] = fr[k] ? fma(beta, p[k], zo) : 0.0;
             s[k] = fma(beta, s[k], w[k]);
-            if (fr[k]) D.pres[i] = fma(alpha, p[k], D.pres[i]);
+            if (fr[k]) {
+                if (xs) xs[k * NT + threadIdx.x] = fma(alpha, p[k], xs[k * NT + threadIdx.x]);
+                else D.pres[i] = fma(alpha, p[k], D.pres[i]);
+            }
             r[k] = fma(-alpha, s[k], r[k]);
             rb[pn][i] = r[k];
             sb[pn][i] = s[k];
@@ -1147,7 +1168,7 @@ __global__ void __launch_bounds__(NT, NT >= 512 ? 1 : 2) k_pcg64c(PcgDev D)
             const int i = row[k];
             if (i < 0) continue;
             const double zi = r[k] * dd[k];
-            w[k] = fr[k] ? fma(D.pdiag[i], zi, off[k]) : 0.0;
+            w[k] = fr[k] ? fma(xs ? pds[k * NT + threadIdx.x] : D.pdiag[i], zi, off[k]) : 0.0;
             wb[pn][i] = w[k];
             if (fr[k]) {
                 if (!isfinite(r[k])) a6.flag = 1.0;
@@ -1158,19 +1179,20 @@ __global__ void __launch_bounds__(NT, NT >= 512 ? 1 : 2) k_pcg64c(PcgDev D)
             }
         }
         t = Acc6{0.0, 0.0, 0.0, 0.0, 0.0};
-        if (!grid_allreduce3<NT>(a6, D, g, phase, t)) return;
+        if (!grid_allreduce3<NT>(a6, D, g, phase, t)) { store_x(); return; }
         ++phase;
         fin = sqrt(t.c);
         mx = t.mx;
         rel = fin / init;
         if (cg_converged(g.conv_test, rel, mx, g.rel_tol, g.abs_tol)) { conv = 1; break; }
-        if (t.flag > 0.0) { if (b == 0 && threadIdx.x == 0) set_status(seg_status(D, g), 4, ST_PCG, it, R_PCG_RESID); return; }
+        if (t.flag > 0.0) { store_x(); if (b == 0 && threadIdx.x == 0) set_status(seg_status(D, g), 4, ST_PCG, it, R_PCG_RESID); return; }
         const double gn = t.a;
-        if (gn <= 1.0e-300 || !isfinite(gn)) { if (b == 0 && threadIdx.x == 0) set_status(seg_status(D, g), 3, ST_PCG, it, R_PCG_RZ); return; }
+        if (gn <= 1.0e-300 || !isfinite(gn)) { store_x(); if (b == 0 && threadIdx.x == 0) set_status(seg_status(D, g), 3, ST_PCG, it, R_PCG_RZ); return; }
         beta = gn / gam;
         den = t.b - beta * gn / alpha;
         gam = gn;
     }
+    store_x();
     if (it > g.max_iter) it = g.max_iter;
     cg_finish(D, g, it, conv, init, fin, rel, mx);
     if (!conv && b == 0 && threadIdx.x == 0) set_status(seg_status(D, g), 2, ST_PCG, it, R_PCG_MAXIT);
@@ -2253,6 +2275,26 @@ void PcgEngine::init(const HostModel& m, const uint8_t* nflag, const double* pfi
             rmax = rm[c];
             nblocks = g;
             halo_smem = smem;
+            // the CG-CG kernel's own rows (pressure, diagonal) in shared
+            // memory: measured faster for the two-CTAs-per-SM kernel of small
+            // meshes (5.2 instead of 5.4 us per iteration at 16^3) and slower
+            // for the one-CTA kernel of large ones (13.4 instead of 13.1 us at
+            // 64^3, where those rows already hit in L1 and a larger shared-
+            // memory carve-out leaves less L1 for the rest)
+            cgcg_smem = smem;
+            cgcg_xs_off = 0;
+            if (want == 4 && nt == 256) {
+                const size_t off = (smem + 15) & ~static_cast<size_t>(15);
+                const size_t with = off + static_cast<size_t>(rm[c]) * nt * 16;
+                int per2 = 0;
+                if (with <= 227 * 1024 && raise_smem_limit(fn, with) == cudaSuccess &&
+                    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per2, fn, nt, with) == cudaSuccess &&
+                    per2 * sms >= g) {
+                    cgcg_smem = with;
+                    cgcg_xs_off = static_cast<int>(off);
+                }
+                cudaGetLastError();
+            }
             d_halo_ptr = dalloc<int>(hptr.size());
             d_halo_idx = dalloc<int>(hidx.size());
             d_lcol = dalloc<unsigned short>(lcol.size());
@@ -2307,6 +2349,7 @@ void PcgEngine::init(const HostModel& m, const uint8_t* nflag, const double* pfi
     dev.slot_max = dev_slot_max;
     dev.part = d_part; dev.bar = d_bar; dev.status = d_status; dev.out = d_out;
     dev.halo_ptr = d_halo_ptr; dev.halo_idx = d_halo_idx; dev.lcol = d_lcol; dev.halo_max = dev_halo_max;
+    dev.xs_off = cgcg_xs_off;
     dev.row_node = d_row_node;
 }
 
@@ -2398,7 +2441,7 @@ cbs3d_status PcgEngine::solve(double* pres, double* rhs1, double* pdiag, int pre
         smem = mixed_smem;
     } else if (variant == 4) {
         fn = fn_cgcg_single(rmax, nthreads);
-        smem = halo_smem;
+        smem = cgcg_smem;
     }
     CoarseDev C = cdev;
     void* args2[] = {&D, &C};

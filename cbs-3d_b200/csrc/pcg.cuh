@@ -64,6 +64,8 @@ struct PcgDev {
     CgOut* out;
     const int* cta_inst;         // batched launch: instance of each CTA (else null)
     const PcgInst* inst;         // batched launch: instance descriptors (else null)
+    int xs_off;                  // CG-CG kernel: byte offset in shared memory of its rows' pressure
+                                 // and diagonal (2*RMAX*threads doubles); 0: read from global memory
 };
 
 // Two-level preconditioner data of one launch: the coarse space is one
@@ -125,6 +127,8 @@ public:
     void coarse_setup(const double* pdiag, const int* row_node, cudaStream_t st);
     int variant = 1;         // 1 global vectors, 2 register rows, 3 + shared-memory halo, 4 + one sync per iteration
     size_t halo_smem = 0;    // dynamic shared memory of the halo kernel
+    size_t cgcg_smem = 0;    // ... of the CG-CG kernel (halo + its rows' pressure and diagonal)
+    int cgcg_xs_off = 0;     // where those rows start (0: kept in global memory)
     size_t mixed_smem = 0;   // dynamic shared memory of the mixed-precision kernel
     bool mixed_ok = false;   // mixed precision runs on the FP32 kernel (else FP64)
     int dev_slot_max = 0;
