@@ -11,6 +11,7 @@
 #include <cstring>
 #include <fstream>
 #include <sstream>
+#include <thread>
 #include <unordered_map>
 
 #include <sys/stat.h>
@@ -96,6 +97,130 @@ struct Scanner {
         return true;
     }
 };
+
+// ------------------------------------------------ parallel section parsing
+// The element and node sections of a large .plt are parsed by several
+// threads when the text holds exactly one record per line: each thread
+// converts the numbers of a range of lines into a staging array in file
+// order, and the records are then placed by their index in one sequential
+// pass (a repeated index keeps the last record, as the sequential reader
+// does).  Any other layout (records spread over lines, blank or comment
+// lines inside a section, too few lines) makes the caller use the sequential
+// scanner instead, so both readers accept and reject the same files.
+
+// the position after n newline-terminated lines, or null if there are fewer
+const char* skip_lines(const char* p, const char* end, size_t n)
+{
+    for (size_t i = 0; i < n; ++i) {
+        const void* q = std::memchr(p, '\n', static_cast<size_t>(end - p));
+        if (!q) return (i + 1 == n && p < end) ? end : nullptr;
+        p = static_cast<const char*>(q) + 1;
+    }
+    return p;
+}
+
+// Numbers of one record per line: NI integers, then ND doubles.  Fills
+// out[line * (NI + ND)] (integers stored as doubles are exact) and returns
+// false if any line does not hold exactly NI + ND numbers.
+template <int NI, int ND>
+bool parse_lines(const char* p, const char* end, size_t nlines, double* out)
+{
+    constexpr int W = NI + ND;
+    unsigned nt = std::max(1u, std::min(16u, std::thread::hardware_concurrency()));
+    if (nlines < 100000) nt = 1;
+    // chunk boundaries on line starts
+    std::vector<const char*> cut(nt + 1, p);
+    cut[nt] = end;
+    for (unsigned t = 1; t < nt; ++t) {
+        const char* c = p + (end - p) * static_cast<long long>(t) / nt;
+        if (c < cut[t - 1]) c = cut[t - 1];
+        const void* q = std::memchr(c, '\n', static_cast<size_t>(end - c));
+        cut[t] = q ? static_cast<const char*>(q) + 1 : end;
+    }
+    std::vector<size_t> first(nt + 1, 0);   // line index of each chunk's start
+    for (unsigned t = 0; t < nt; ++t) {
+        size_t n = 0;
+        for (const char* c = cut[t]; c < cut[t + 1];) {
+            const void* q = std::memchr(c, '\n', static_cast<size_t>(cut[t + 1] - c));
+            ++n;
+            c = q ? static_cast<const char*>(q) + 1 : cut[t + 1];
+        }
+        first[t + 1] = first[t] + n;
+    }
+    if (first[nt] != nlines) return false;
+    std::vector<char> ok(nt, 1);
+    auto work = [&](unsigned t) {
+        const char* c = cut[t];
+        const char* stop = cut[t + 1];
+        double* o = out + first[t] * W;
+        while (c < stop) {
+            const char* eol = static_cast<const char*>(std::memchr(c, '\n', static_cast<size_t>(stop - c)));
+            if (!eol) eol = stop;
+            for (int k = 0; k < W; ++k) {
+                while (c < eol && std::isspace(static_cast<unsigned char>(*c))) ++c;
+                if (c >= eol) { ok[t] = 0; return; }
+                char* q = nullptr;
+                if (k < NI) {
+                    errno = 0;
+                    const long x = std::strtol(c, &q, 10);
+                    if (q == c || errno || q > eol) { ok[t] = 0; return; }
+                    o[k] = static_cast<double>(static_cast<int>(x));
+                } else {
+                    const double x = std::strtod(c, &q);
+                    if (q == c || q > eol) { ok[t] = 0; return; }
+                    o[k] = x;
+                }
+                c = q;
+            }
+            while (c < eol && std::isspace(static_cast<unsigned char>(*c))) ++c;
+            if (c != eol) { ok[t] = 0; return; }
+            c = eol < stop ? eol + 1 : stop;
+            o += W;
+        }
+    };
+    if (nt == 1) {
+        work(0);
+    } else {
+        std::vector<std::thread> th;
+        for (unsigned t = 0; t < nt; ++t) th.emplace_back(work, t);
+        for (auto& x : th) x.join();
+    }
+    for (char x : ok)
+        if (!x) return false;
+    return true;
+}
+
+// The element and node sections of a large regular .plt (see above); on
+// success the records are placed with the sequential reader's checks and
+// messages, in file order, and sc points past the node section.
+bool parse_sections_parallel(HostModel& m, Scanner& sc)
+{
+    const size_t E = static_cast<size_t>(m.E), N = static_cast<size_t>(m.N);
+    if (E + N < 100000) return false;
+    const char* e_end = skip_lines(sc.p, sc.end, E);
+    const char* n_end = e_end ? skip_lines(e_end, sc.end, N) : nullptr;
+    if (!n_end) return false;
+    std::vector<double> ev(E * 5), nv(N * 4);
+    if (!parse_lines<5, 0>(sc.p, e_end, E, ev.data()) || !parse_lines<1, 3>(e_end, n_end, N, nv.data())) return false;
+    for (size_t i = 0; i < E; ++i) {
+        const double* r = &ev[5 * i];
+        const int ie = static_cast<int>(r[0]);
+        if (ie < 1 || ie > m.E) bad("MeshIO::readMeshFile - element index out of range");
+        for (int j = 0; j < 4; ++j) {
+            const int v = static_cast<int>(r[1 + j]);
+            if (v < 1 || v > m.N) bad("MeshIO::readMeshFile - connectivity node out of range");
+            m.intma[4 * static_cast<size_t>(ie - 1) + j] = v;
+        }
+    }
+    for (size_t i = 0; i < N; ++i) {
+        const double* r = &nv[4 * i];
+        const int ip = static_cast<int>(r[0]);
+        if (ip < 1 || ip > m.N) bad("MeshIO::readMeshFile - node index out of range");
+        for (int j = 0; j < 3; ++j) m.coord[3 * static_cast<size_t>(ip - 1) + j] = r[1 + j];
+    }
+    sc.p = n_end;
+    return true;
+}
 
 // skip the first data line (header) of a buffer, returning a pointer past it
 const char* after_first_data_line(const std::string& buf, std::string& header)
@@ -493,24 +618,26 @@ void parse_case(const std::string& case_name, HostModel& m)
     m.coord.assign(3 * N, 0.0);
     m.iside.assign(6 * NB, 0);
     Scanner sc{body, plt.data() + plt.size()};
-    for (size_t i = 0; i < E; ++i) {
-        int ie = 0;
-        if (!sc.next_int(ie)) bad("MeshIO::readMeshFile - cannot read element index");
-        if (ie < 1 || ie > m.E) bad("MeshIO::readMeshFile - element index out of range");
-        for (int j = 0; j < 4; ++j) {
-            int v = 0;
-            if (!sc.next_int(v)) bad("MeshIO::readMeshFile - cannot read tetrahedral connectivity");
-            if (v < 1 || v > m.N) bad("MeshIO::readMeshFile - connectivity node out of range");
-            m.intma[4 * static_cast<size_t>(ie - 1) + j] = v;
+    if (!parse_sections_parallel(m, sc)) {
+        for (size_t i = 0; i < E; ++i) {
+            int ie = 0;
+            if (!sc.next_int(ie)) bad("MeshIO::readMeshFile - cannot read element index");
+            if (ie < 1 || ie > m.E) bad("MeshIO::readMeshFile - element index out of range");
+            for (int j = 0; j < 4; ++j) {
+                int v = 0;
+                if (!sc.next_int(v)) bad("MeshIO::readMeshFile - cannot read tetrahedral connectivity");
+                if (v < 1 || v > m.N) bad("MeshIO::readMeshFile - connectivity node out of range");
+                m.intma[4 * static_cast<size_t>(ie - 1) + j] = v;
+            }
         }
-    }
-    for (size_t i = 0; i < N; ++i) {
-        int ip = 0;
-        if (!sc.next_int(ip)) bad("MeshIO::readMeshFile - cannot read node index");
-        if (ip < 1 || ip > m.N) bad("MeshIO::readMeshFile - node index out of range");
-        for (int j = 0; j < 3; ++j)
-            if (!sc.next_double(m.coord[3 * static_cast<size_t>(ip - 1) + j]))
-                bad("MeshIO::readMeshFile - cannot read 3D coordinate");
+        for (size_t i = 0; i < N; ++i) {
+            int ip = 0;
+            if (!sc.next_int(ip)) bad("MeshIO::readMeshFile - cannot read node index");
+            if (ip < 1 || ip > m.N) bad("MeshIO::readMeshFile - node index out of range");
+            for (int j = 0; j < 3; ++j)
+                if (!sc.next_double(m.coord[3 * static_cast<size_t>(ip - 1) + j]))
+                    bad("MeshIO::readMeshFile - cannot read 3D coordinate");
+        }
     }
     for (size_t ib = 0; ib < NB; ++ib) {
         int n1, n2, n3, parent, raw;

@@ -190,3 +190,34 @@ def test_abi_rejects_bad_inputs_before_touching_a_device():
     assert L.cbs3d_coarse_inverse(0, 165, gpu._ptr(m), gpu._ptr(out), 1) == 1
     assert L.cbs3d_coarse_inverse(0, 3, gpu._ptr(m), gpu._ptr(out), 2) == 1
     assert L.cbs3d_coarse_inverse(0, 3, None, gpu._ptr(out), 0) == 1
+
+
+def test_parallel_section_parse_matches_sequential(tmp_path):
+    """Large .plt files with one record per line are parsed by several
+    threads; any other layout goes through the sequential scanner.  Both
+    must give the same inputs and the same error for the same records."""
+    from cbs3d import cases, gpu
+    base = cases.cavity(32, ntime=5).write(str(tmp_path), "reg")   # 196,608 tets + 35,937 nodes
+    plt = open(base + ".plt").read().split("\n")
+    # the same records with the first element spread over two lines: sequential path
+    alt = plt[:]
+    first = alt[1].split()
+    alt[1] = " ".join(first[:2]) + "\n" + " ".join(first[2:])
+    alt_base = str(tmp_path / "alt")
+    for ext in (".bco", ".par"):
+        open(alt_base + ext, "w").write(open(base + ext).read())
+    open(alt_base + ".plt", "w").write("\n".join(alt))
+    d_par, _ = gpu.case_digest(base, use_cache=False)
+    d_seq, _ = gpu.case_digest(alt_base, use_cache=False)
+    assert d_par == d_seq
+    # a node index out of range in element 1000, in both layouts
+    for b, lines in ((base, plt), (alt_base, alt)):
+        bad = lines[:]
+        k = 1000 + (1 if b == alt_base else 0)
+        t = bad[k].split()
+        t[3] = str(10 ** 8)
+        bad[k] = " ".join(t)
+        open(b + ".plt", "w").write("\n".join(bad))
+        with pytest.raises(gpu.CBSError) as e:
+            gpu.case_digest(b, use_cache=False)
+        assert "connectivity node out of range" in e.value.message
