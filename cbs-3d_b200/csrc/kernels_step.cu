@@ -318,7 +318,34 @@ __global__ void k_lhs(DevState S)
     if (i >= S.P.N) return;
     const int E = S.P.E;
     double s2 = 0.0, s2p = 0.0, pd = 0.0;
-    for (int k = S.n2e_ptr[i]; k < S.n2e_ptr[i + 1]; ++k) {
+    // incident elements in order, their data loaded four at a time
+    const int kb = S.n2e_ptr[i], ke = S.n2e_ptr[i + 1];
+    int k = kb;
+    for (; k + 4 <= ke; k += 4) {
+        int ent[4];
+        double dt[4], dj[4], rc[4], pe[4];
+        bool fl[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) ent[u] = S.n2e[k + u];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            const int e = ent[u] >> 2, a = ent[u] & 3;
+            dt[u] = S.delte[e];
+            dj[u] = S.detJ[e];
+            fl[u] = S.mat[e] == 0;
+            rc[u] = S.rho_cp[e];
+            pe[u] = S.pdiagE[(size_t)a * E + e];
+        }
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            if (dt[u] <= 0.0 || !isfinite(dt[u])) { set_status(S.status, 1, ST_LHS, (ent[u] >> 2) + 1, R_LHS_DT); return; }
+            const double mass = dj[u] * MASS_FACTOR;
+            if (fl[u]) s2 += mass / dt[u];
+            s2p += rc[u] * mass / dt[u];
+            if (fl[u]) pd += pe[u] * dt[u];
+        }
+    }
+    for (; k < ke; ++k) {
         const int e = S.n2e[k] >> 2, a = S.n2e[k] & 3;
         const double dt = S.delte[e];
         if (dt <= 0.0 || !isfinite(dt)) { set_status(S.status, 1, ST_LHS, e + 1, R_LHS_DT); return; }
@@ -577,7 +604,27 @@ __global__ void k_step1_node(DevState S)
     if (i >= S.P.N) return;
     const int E = S.P.E;
     double r0 = 0.0, r1 = 0.0, r2 = 0.0;
-    for (int k = S.n2c_ptr[i]; k < S.n2c_ptr[i + 1]; ++k) {
+    // colour order, records loaded four at a time
+    const int kb = S.n2c_ptr[i], ke = S.n2c_ptr[i + 1];
+    int k = kb;
+    for (; k + 4 <= ke; k += 4) {
+        double x0[4], x1[4], x2[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            const int ent = S.n2c[k + u];
+            const int e = ent >> 2, a = ent & 3;
+            x0[u] = S.elbuf[(size_t)(0 * 4 + a) * E + e];
+            x1[u] = S.elbuf[(size_t)(1 * 4 + a) * E + e];
+            x2[u] = S.elbuf[(size_t)(2 * 4 + a) * E + e];
+        }
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            r0 += x0[u];
+            r1 += x1[u];
+            r2 += x2[u];
+        }
+    }
+    for (; k < ke; ++k) {
         const int e = S.n2c[k] >> 2, a = S.n2c[k] & 3;
         r0 += S.elbuf[(size_t)(0 * 4 + a) * E + e];
         r1 += S.elbuf[(size_t)(1 * 4 + a) * E + e];
@@ -650,7 +697,23 @@ __global__ void k_step2_node(DevState S)
     if (i >= S.P.N) return;
     const int E = S.P.E;
     double r = 0.0;
-    for (int k = S.n2e_ptr[i]; k < S.n2e_ptr[i + 1]; ++k) {
+    const int kb = S.n2e_ptr[i], ke = S.n2e_ptr[i + 1];
+    int k = kb;
+    for (; k + 4 <= ke; k += 4) {
+        double x[4];
+        bool fl[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            const int ent = S.n2e[k + u];
+            const int e = ent >> 2, a = ent & 3;
+            fl[u] = S.mat[e] == 0;
+            x[u] = S.elbuf[(size_t)a * E + e];
+        }
+#pragma unroll
+        for (int u = 0; u < 4; ++u)
+            if (fl[u]) r += x[u];
+    }
+    for (; k < ke; ++k) {
         const int e = S.n2e[k] >> 2, a = S.n2e[k] & 3;
         if (S.mat[e] != 0) continue;
         r += S.elbuf[(size_t)a * E + e];
@@ -685,7 +748,28 @@ __global__ void k_step3_node(DevState S)
     if (i >= S.P.N) return;
     const int E = S.P.E;
     double r0 = 0.0, r1 = 0.0, r2 = 0.0;
-    for (int k = S.n2e_ptr[i]; k < S.n2e_ptr[i + 1]; ++k) {
+    const int kb = S.n2e_ptr[i], ke = S.n2e_ptr[i + 1];
+    int k = kb;
+    for (; k + 4 <= ke; k += 4) {
+        double x0[4], x1[4], x2[4];
+        bool fl[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            const int e = S.n2e[k + u] >> 2;
+            fl[u] = S.mat[e] == 0;
+            x0[u] = S.elbuf[(size_t)0 * E + e];
+            x1[u] = S.elbuf[(size_t)1 * E + e];
+            x2[u] = S.elbuf[(size_t)2 * E + e];
+        }
+#pragma unroll
+        for (int u = 0; u < 4; ++u)
+            if (fl[u]) {
+                r0 -= x0[u];
+                r1 -= x1[u];
+                r2 -= x2[u];
+            }
+    }
+    for (; k < ke; ++k) {
         const int e = S.n2e[k] >> 2;
         if (S.mat[e] != 0) continue;
         r0 -= S.elbuf[(size_t)0 * E + e];
