@@ -221,3 +221,21 @@ def test_parallel_section_parse_matches_sequential(tmp_path):
         with pytest.raises(gpu.CBSError) as e:
             gpu.case_digest(b, use_cache=False)
         assert "connectivity node out of range" in e.value.message
+
+
+def test_bench_reference_arm_contract():
+    """bench.py --impl reference times the reference's own OpenMP build on
+    the host cores and prints the same metric with impl=reference."""
+    import json
+    import subprocess
+    import sys
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    if not os.path.exists(os.path.join(root, "oracle", "_ref", "cbs_ref_harness")):
+        pytest.skip("reference harness not built")
+    r = subprocess.run([sys.executable, os.path.join(root, "bench.py"), "--impl", "reference", "--steps", "1",
+                        "--warmup", "0"], cwd=root, capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, r.stderr[-2000:]
+    d = json.loads([l for l in r.stdout.splitlines() if l.startswith("{")][-1])
+    assert d["impl"] == "reference" and d["value"] > 0 and d["unit"] == "steps/s"
+    assert d["cpu_baseline"]["kind"] == "reference" and d["cpu_baseline"]["cores"] >= 1
+    assert d["e2e"]["h2d_bytes_per_step"] == 0 and d["e2e"]["value"] == d["value"]
