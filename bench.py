@@ -387,6 +387,20 @@ def arm_batch(args):
     info = b.info()
     launches = int(sum(x.kernel_launches for x in st))
     b.close()
+    # the same batch with FP32 inner solves and FP64 residual replacement
+    # (the batched configuration's solver), timed the same way
+    mixed = None
+    if args.precision == "both":
+        bm = gpu.Batch(mine, precision=gpu.MIXED, device=local, autotune=True)
+        bm.step(max(args.warmup, 1))
+        barrier(dist)
+        mst, msec = bm.step(args.steps)
+        barrier(dist)
+        msec = dist_max(dist, msec)
+        mixed = {"value": len(cs) * args.steps / msec, "unit": "instance-steps/s",
+                 "ms_per_step": 1e3 * msec / args.steps, "speedup_vs_fp64": sec / msec,
+                 "batch_rank0": bm.info(), "gpu_launches": int(sum(x.kernel_launches for x in mst))}
+        bm.close()
     if rank == 0:
         print(json.dumps({
             "metric": "CBS instance-steps/s, 48 batched cavities", "value": len(cs) * args.steps / sec,
@@ -397,7 +411,7 @@ def arm_batch(args):
                                    "50..1000, seed 2024, Jacobi-PCG relTol 1e-8, one batched step per CUDA graph",
                        "nelem_total": int(sum(c.mesh.nelem for c in cs)), "parallelism": f"LPT shards x{ws}",
                        "l2": "inputs larger than L2 (no flush)"},
-            "batch_rank0": info, "gpu_launches": launches, "clocks": clk}))
+            "batch_rank0": info, "gpu_launches": launches, "clocks": clk, "mixed": mixed}))
     if dist is not None:
         barrier(dist)
         dist.destroy_process_group()
