@@ -1118,8 +1118,8 @@ __global__ void __launch_bounds__(NT, NT >= 512 ? 1 : 2) k_pcg64c(PcgDev D)
         alpha = gam / den;
         const int po = (it - 1) & 1, pn = it & 1;
         // stage z_it of the halo: s = w_o + beta*s_o, r = r_o - alpha*s, z = r / dz
-        // (SU halo nodes per thread per round, all their loads issued first)
-        __syncthreads();
+        // (SU halo nodes per thread per round, all their loads issued first);
+        // the all-reduce above ended with a barrier, so vh is free to write
         {
             constexpr int SU = 4;
             const double* so = sb[po];
