@@ -913,7 +913,7 @@ __global__ void k_conv_partial(DevState S)
             v[10] = S.pres[i] * S.pres[i];
             v[11] = dl * dl;
         }
-        if (S.P.temp_calc > 0) {
+        if (S.P.temp_calc > 0 && (tf || ts)) {   // thermal_active (Convergence.cpp:178)
             const double dl = S.temp[i] - S.temp1[i];
             v[12] = dl * dl;
             v[13] = S.temp[i] * S.temp[i];

@@ -272,15 +272,22 @@ const char* cbs3d_pcg_last_error(const cbs3d_pcg* pcg);
  * device arrays the caller already holds (node-major unkno/unkn1[3*npoin],
  * pres/pres1/temperature/temperature1/elcoe2/elcoe2p[npoin];
  * node_flags[npoin]: bit0 = node touches a fluid element, bit1 = touches a
- * solid element).  For callers that may not call cudaMalloc -- e.g. a host
- * loop that must not stall the device or a process whose device memory is
- * owned by another allocator: the only scratch is a 1 MiB file-scope device
- * array that every GPU loading this library holds until exit.  npoin above
- * 2,097,152 is rejected with CBS3D_INVALID_INPUT.  The first call on a device
- * looks up that array's device address; make that first call before any
- * stream capture.  All calls share the array: calls whose kernels overlap on
- * the GPU race.  Runs on the legacy default stream and returns when hb is on
- * the host. */
+ * solid element; the temperature arrays may be NULL when temp_calc <= 0).
+ * For callers that may not call cudaMalloc -- code whose device memory is
+ * owned by another allocator (a framework's caching allocator, a pool handed
+ * out by an embedding application) or a process that budgeted its device
+ * memory up front: the only scratch is a 1 MiB file-scope device array that
+ * every GPU loading this library holds until exit.  npoin above 2,097,152 is
+ * rejected with CBS3D_INVALID_INPUT, and so is a node whose flags are 0
+ * (touches no element), as Convergence::evaluate rejects it
+ * (src/solver/Convergence.cpp:157-161).  The first call on a device looks up
+ * that array's device address; make that first call before any stream
+ * capture, and do not call it again after a cudaDeviceReset of that device.
+ * All calls share the array: calls whose kernels overlap on the GPU race.
+ * The kernels run on the legacy default stream and the call blocks the host
+ * until hb is copied back, so finish or synchronise every stream that writes
+ * the inputs (this library's context streams are non-blocking) before the
+ * call.  The caller's current device is restored on return. */
 cbs3d_status cbs3d_convergence_norms_static(int device, const double* unkno, const double* unkn1,
                                             const double* pres, const double* pres1,
                                             const double* temperature, const double* temperature1,

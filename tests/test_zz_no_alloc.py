@@ -1,13 +1,15 @@
 """The allocation-free entry point cbs3d_convergence_norms_static.
 
-It exists for callers that cannot call cudaMalloc (a host loop that must not
-stall the device, or a process whose device memory belongs to another
-allocator); its only scratch is a file-scope device array.  This test feeds it
-device copies of a context's state and compares its measures with the ones the
-engine's own convergence kernels produced, on two calls in a row, so a second
-call over the shared scratch must not see the first call's leftovers.  The
-file sorts last so that a run stopping at the first failure has already run
-every other test."""
+It exists for callers that cannot call cudaMalloc (a process whose device
+memory belongs to another allocator, or one that budgeted its device memory
+up front); its only scratch is a file-scope device array shared by every
+call.  This test feeds it device copies of a context's state and requires the
+engine's own convergence measures bit for bit, on calls in a row: a
+two-block conjugate-heat-transfer case with the energy equation on, then a
+one-block cavity with the energy equation off and no temperature arrays (a
+call that read the first call's leftover partials would differ), then the
+first case again.  The file sorts last so that a run stopping at the first
+failure has already run every other test."""
 import ctypes
 
 import numpy as np
@@ -37,24 +39,53 @@ def _node_flags(case) -> np.ndarray:
     return flags
 
 
-def test_static_scratch_norms_match_engine_on_two_calls():
+def _state(name):
+    """A context one step in, its engine measures and device copies of the
+    fields the entry point reads (temperature left out when it is off)."""
     import torch
 
     from cbs3d import gpu
-    case, _ = load_case(fixture_path("cht"))      # fluid + solid nodes, energy on
+    case, _ = load_case(fixture_path(name))
     ctx = gpu.Context(case)
+    ctx.step(1)
+    temp = case.params.get("temp_calc", 0) > 0
+    dev = {n: torch.tensor(ctx.get(n), dtype=torch.float64, device="cuda")
+           for n in FIELDS if temp or not n.startswith("temperature")}
     flags = torch.tensor(_node_flags(case), dtype=torch.uint8, device="cuda")
+    torch.cuda.synchronize()
+    return ctx, dev, flags, int(temp)
+
+
+def _call(fn, dev, flags, npoin, temp):
+    ptr = [ctypes.c_void_p(dev[n].data_ptr()) if n in dev else None for n in FIELDS]
+    hb = (ctypes.c_double * 15)()
+    rc = fn(0, *ptr, ctypes.c_void_p(flags.data_ptr()), npoin, temp, hb)
+    return rc, np.array(hb[:])
+
+
+def test_static_scratch_norms_match_engine_on_calls_in_a_row():
+    import torch
     fn = _entry()
-    for _ in range(2):
-        ctx.step(1)
+    big = _state("cht")        # 315 nodes: two blocks of partials, energy on
+    small = _state("cav4")     # 125 nodes: one block, energy off
+    assert big[0].npoin > 256 >= small[0].npoin
+    for ctx, dev, flags, temp in (big, small, big):
         want = ctx.get("hb")
-        dev = {n: torch.tensor(ctx.get(n), dtype=torch.float64, device="cuda") for n in FIELDS}
-        torch.cuda.synchronize()
-        hb = (ctypes.c_double * 15)()
-        rc = fn(0, *[ctypes.c_void_p(dev[n].data_ptr()) for n in FIELDS], ctypes.c_void_p(flags.data_ptr()),
-                ctx.npoin, 1, hb)
+        dev_before = torch.cuda.current_device()
+        rc, hb = _call(fn, dev, flags, ctx.npoin, temp)
         assert rc == 0
-        np.testing.assert_allclose(np.array(hb[:]), want, rtol=1e-12, atol=1e-300)
+        assert torch.cuda.current_device() == dev_before
+        assert np.array_equal(hb, want), (hb, want)
+        if not temp:
+            assert np.all(hb[12:15] == 0.0)
+
+
+def test_static_scratch_rejects_orphan_node():
+    fn = _entry()
+    ctx, dev, flags, temp = _state("cav4")
+    flags[7] = 0                # a node that touches no element
+    rc, _ = _call(fn, dev, flags, ctx.npoin, temp)
+    assert rc == 1
 
 
 def test_static_scratch_rejects_oversize():
