@@ -15,15 +15,25 @@ and node data, far more than the 126 MB L2, so no flush is inserted.
 `value` is the FP64 engine with the reference's Jacobi-PCG (the drop-in for
 the reference's FP64 path); with --precision both (the default) the same
 line carries the mixed engine (FP32 inner PCG, FP64 defect correction) under
-"mixed" and the FP64 engine with the two-level preconditioner (Jacobi plus a
-per-CTA coarse correction, same stopping test) under "two_level": their
-steps/s and relative L2 errors on u and p against the Jacobi FP64 engine
-after the same steps.
+"mixed", the FP64 engine with the aggregation-multigrid preconditioner
+(same stopping test) under "multigrid" and with the per-CTA two-level
+preconditioner under "two_level": their steps/s and relative L2 errors on u
+and p against the Jacobi FP64 engine after the same steps.  "batch" holds
+the 48-cavity batched step (instance-steps/s, FP64 and mixed, against the
+same instances stepped one after another).
 
-Roofline of the PCG kernel: algorithmic bytes per iteration are the
-element-by-element operator's traffic, 64*E_f + 73*N in FP64 and
-40*E_f + 37*N in FP32 (E_f fluid tets, N nodes), times the iterations one
-launch (one pressure solve) runs, over the launch's CUDA-event duration.
+Rooflines of the PCG kernel.  Bytes per iteration are the implemented
+kernel's (the assembled SELL operator's coefficients and columns plus its
+per-node vector traffic, cbs3d_step_stats.pcg_bytes_per_iter); the
+element-by-element form's 64*E_f + 73*N (FP64) is reported beside them for
+context only, since the assembled operator moves fewer bytes.  achieved =
+bytes per iteration x iterations / the PCG launches' CUDA-event time.  At
+64^3 the operator and vectors (~50 MB) stay in the 126 MB L2, so "roofline"
+is stated against the L2 copy bandwidth measured in this run (a copy of a
+2 x 24 MiB buffer pair, cbs3d_probe_copy_bandwidth), with the grid
+all-reduce latency (cbs3d_probe_allreduce) as the per-iteration floor;
+"hbm_case" runs the same FP64 engine on a 96^3 cavity, whose per-iteration
+traffic exceeds L2, against the measured HBM copy bandwidth.
 
 Multi-GPU: the single-case path does not shard (replicas only); each rank
 runs its own replica and `value` is the total steps/s of all ranks.
@@ -62,6 +72,9 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--workload", default="cavity64", choices=["cavity64", "batch"],
                     help="batch: 48 seeded cavities of 10..40 hexes per side, Re 50..1000, batched step")
+    ap.add_argument("--hbm-n", type=int, default=96, help="hexes per side of the HBM-bound PCG case (0: skip)")
+    ap.add_argument("--hbm-steps", type=int, default=3)
+    ap.add_argument("--batch-steps", type=int, default=10, help="timed steps of the batch key (0: skip)")
     return ap.parse_args()
 
 
@@ -134,6 +147,27 @@ def measured_peak():
             d = json.load(f)
         return float(d["hbm_gbs"]), "measured"
     return 6650.0, "fallback"
+
+
+def probes(device: int) -> dict:
+    """L2 and HBM copy bandwidth and the grid all-reduce latency on this GPU,
+    measured with the library's probe kernels (CUDA events)."""
+    import ctypes
+
+    from cbs3d import gpu
+    L = gpu.lib()
+    L.cbs3d_probe_copy_bandwidth.argtypes = [ctypes.c_int, ctypes.c_longlong, ctypes.c_int,
+                                             ctypes.POINTER(ctypes.c_double)]
+    L.cbs3d_probe_allreduce.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_double)]
+    l2, hbm, ar = ctypes.c_double(), ctypes.c_double(), ctypes.c_double()
+    out = {}
+    if L.cbs3d_probe_copy_bandwidth(device, 24 << 20, 100, ctypes.byref(l2)) == 0:
+        out["l2_copy_gbs"] = l2.value
+    if L.cbs3d_probe_copy_bandwidth(device, 1 << 30, 10, ctypes.byref(hbm)) == 0:
+        out["hbm_copy_gbs"] = hbm.value
+    if L.cbs3d_probe_allreduce(device, 4000, ctypes.byref(ar)) == 0:
+        out["allreduce_us"] = ar.value
+    return out
 
 
 def ncu_traffic(kernel: str, n: int):
@@ -235,12 +269,15 @@ def arm_reference(args):
         dist.destroy_process_group()
 
 
-def algorithmic_bytes(nelem_fluid: int, npoin: int, mixed: bool) -> int:
-    """Bytes one PCG iteration of the element-by-element Jacobi-PCG moves:
+def ebe_bytes(nelem_fluid: int, npoin: int, mixed: bool) -> int:
+    """Bytes one PCG iteration of the element-by-element form would move:
     per fluid tet 4 int32 connectivity + 6 coefficients, per node p, Ap
     (written and read), pres and r (read and written), pdiag, new p, plus a
     one-byte mask -- FP64 64*E_f + 73*N, FP32 inner 40*E_f + 37*N."""
     return (40 * nelem_fluid + 37 * npoin) if mixed else (64 * nelem_fluid + 73 * npoin)
+
+
+KERNELS = {1: "k_pcg64", 2: "k_pcg64r", 3: "k_pcg64h", 4: "k_pcg64c", 5: "k_pcg32m", 6: "k_pcg64d", 7: "k_pcg_mg"}
 
 
 def timed_run(args, ctx, dist):
@@ -255,20 +292,86 @@ def timed_run(args, ctx, dist):
     return warm, st, sec, clocks.stop()
 
 
-def roofline(st, warm, nelem_fluid, npoin, mixed, n):
-    peak, peak_kind = measured_peak()
+def roofline(st, warm, nelem_fluid, npoin, mixed, n, pr, bound="l2"):
+    """PCG kernel roofline: the kernel's own bytes per iteration over its
+    CUDA-event time, against the L2 copy bandwidth measured in this run
+    (bound "l2": the solve's operator and vectors stay in L2) or the
+    measured HBM copy bandwidth (bound "hbm")."""
+    hbm, hbm_kind = measured_peak()
     its = st.cg_iterations_total - warm.cg_iterations_total   # totals are cumulative
-    alg = algorithmic_bytes(nelem_fluid, npoin, mixed)
-    achieved = its * alg / st.pcg_seconds / 1e9 if st.pcg_seconds > 0 else None
-    names = {1: "k_pcg64", 2: "k_pcg64r", 3: "k_pcg64h", 4: "k_pcg64c", 5: "k_pcg32m", 6: "k_pcg64d"}
-    kname = names.get(st.pcg_kernel, "?")
-    return {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-            "frac": achieved / peak if achieved else None, "traffic": ncu_traffic(kname, n),
-            "traffic_unit": "bytes per launch (one pressure solve)",
-            "kernel": f"{kname} (persistent PCG, one launch per pressure solve)",
-            "peak_source": peak_kind, "algorithmic_bytes_per_iteration": alg,
-            "kernel_bytes_per_iteration": st.pcg_bytes_per_iter, "iterations": its,
-            "launches": st.pcg_launches, "avg_launch_ms": 1e3 * st.pcg_seconds / max(st.pcg_launches, 1)}
+    kb = float(st.pcg_bytes_per_iter)
+    achieved = its * kb / st.pcg_seconds / 1e9 if st.pcg_seconds > 0 and its > 0 else None
+    kname = KERNELS.get(st.pcg_kernel, "?")
+    if bound == "l2":
+        peak = pr.get("l2_copy_gbs")
+        src = ("measured in this run: copy of a 2 x 24 MiB L2-resident buffer pair "
+               "(cbs3d_probe_copy_bandwidth, CUDA events)")
+    else:
+        peak, src = hbm, hbm_kind
+    out = {"bound": bound, "achieved": achieved, "peak": peak, "unit": "GB/s",
+           "frac": achieved / peak if achieved and peak else None, "traffic": ncu_traffic(kname, n),
+           "traffic_unit": "DRAM bytes per launch (one pressure solve), ncu",
+           "kernel": f"{kname} (persistent PCG, one launch per pressure solve)", "peak_source": src,
+           "kernel_bytes_per_iteration": kb, "ebe_bytes_per_iteration": ebe_bytes(nelem_fluid, npoin, mixed),
+           "iterations": its, "us_per_iteration": 1e6 * st.pcg_seconds / its if its > 0 else None,
+           "launches": st.pcg_launches, "avg_launch_ms": 1e3 * st.pcg_seconds / max(st.pcg_launches, 1)}
+    if bound == "l2":
+        out["hbm_peak"] = hbm
+        out["hbm_peak_source"] = hbm_kind
+        out["hbm_frac"] = achieved / hbm if achieved else None
+        out["allreduce_us"] = pr.get("allreduce_us")
+    return out
+
+
+def hbm_case(args, local, dist):
+    """The FP64 Jacobi engine on a cavity whose PCG traffic per iteration
+    exceeds L2 (96^3 by default): the PCG roofline against HBM."""
+    from cbs3d import gpu
+    n = args.hbm_n
+    case = make_case(n, ntime=10 ** 6)
+    ctx = gpu.Context(case, precision=gpu.FP64, device=local, use_graph=False, time_pcg=True)
+    warm = ctx.step(1)
+    barrier(dist)
+    st = ctx.step(args.hbm_steps)
+    barrier(dist)
+    sec = dist_max(dist, st.gpu_seconds)
+    roof = roofline(st, warm, case.mesh.nelem, ctx.npoin, False, n, {}, bound="hbm")
+    ctx.close()
+    roof.update({"workload": workload(n), "nelem": case.mesh.nelem, "npoin": case.mesh.npoin,
+                 "steps": args.hbm_steps, "steps_per_s": args.hbm_steps / sec,
+                 "pcg_share_of_step": st.pcg_seconds / st.gpu_seconds if st.gpu_seconds > 0 else None})
+    return roof
+
+
+def batch_key(args, local, dist):
+    """The 48-cavity batch (pressure solves to 1e-8), FP64 and mixed, against
+    the same instances stepped one after another on single contexts."""
+    from cbs3d import cases, gpu
+    cs = cases.cavity_batch()
+    out = {"workload": "48 lid-driven cavities, 10..40 hexes per side x 6 Kuhn tets, Re log-uniform 50..1000, "
+                       "seed 2024, Jacobi-PCG relTol 1e-8, one batched step per CUDA graph",
+           "instances": len(cs), "nelem_total": int(sum(c.mesh.nelem for c in cs)), "steps": args.batch_steps,
+           "unit": "instance-steps/s"}
+    for name, prec in (("fp64", gpu.FP64), ("mixed", gpu.MIXED)):
+        b = gpu.Batch(cs, precision=prec, device=local, autotune=True)
+        b.step(max(args.warmup, 1))            # the autotuner runs in the first step
+        barrier(dist)
+        st, sec = b.step(args.batch_steps)
+        barrier(dist)
+        sec = dist_max(dist, sec)
+        out[name] = {"value": len(cs) * args.batch_steps / sec, "ms_per_step": 1e3 * sec / args.batch_steps,
+                     "autotuned": b.info(), "gpu_launches": int(sum(x.kernel_launches for x in st))}
+        b.close()
+    seq = 0.0
+    for c in cs:
+        ctx = gpu.Context(c, precision=gpu.FP64, device=local)
+        ctx.step(1)
+        seq += ctx.step(args.batch_steps).gpu_seconds
+        ctx.close()
+    out["sequential_fp64_ms_per_step"] = 1e3 * seq / args.batch_steps
+    out["speedup_fp64_vs_sequential"] = out["sequential_fp64_ms_per_step"] / out["fp64"]["ms_per_step"]
+    out["mixed_vs_fp64"] = out["mixed"]["value"] / out["fp64"]["value"]
+    return out
 
 
 def arm_gpu(args):
@@ -277,11 +380,12 @@ def arm_gpu(args):
     case = make_case(args.n, ntime=10 ** 6)
     nelem_fluid = case.mesh.nelem          # the cavity is all fluid
     first = gpu.MIXED if args.precision == "mixed" else gpu.FP64
+    pr = probes(local)
     ctx = gpu.Context(case, precision=first, device=local, use_graph=False, time_pcg=True)
     N = ctx.npoin
     warm, st, sec, clk = timed_run(args, ctx, dist)
     value = ws * args.steps / sec
-    roof = roofline(st, warm, nelem_fluid, N, first == gpu.MIXED, args.n)
+    roof = roofline(st, warm, nelem_fluid, N, first == gpu.MIXED, args.n, pr)
     u0, p0, _ = ctx.fields()
 
     # end to end through the public API with host buffers: upload the state,
@@ -309,6 +413,24 @@ def arm_gpu(args):
     pcg_share = st.pcg_seconds / st.gpu_seconds if st.gpu_seconds > 0 else None
     ctx.close()
 
+    def fp64_variant(**kw):
+        vctx = gpu.Context(case, precision=gpu.FP64, device=local, use_graph=False, time_pcg=True, **kw)
+        vwarm, vst, vsec, _ = timed_run(args, vctx, dist)
+        uv, pv, _ = vctx.fields()
+        out = {"value": ws * args.steps / vsec, "unit": "steps/s", "ms_per_step": 1e3 * vsec / args.steps,
+               "speedup_vs_fp64": (ws * args.steps / vsec) / value, "pcg_kernel": int(vst.pcg_kernel),
+               "rel_l2_u_vs_fp64": float(np.linalg.norm(uv - u0) / np.linalg.norm(u0)),
+               "rel_l2_p_vs_fp64": float(np.linalg.norm(pv - p0) / np.linalg.norm(p0)),
+               "pcg_iterations_per_step": (vst.cg_iterations_total - vwarm.cg_iterations_total) / args.steps,
+               "pcg_share_of_step": vst.pcg_seconds / vst.gpu_seconds if vst.gpu_seconds > 0 else None,
+               "gpu_launches": int(vst.kernel_launches),
+               "roofline": roofline(vst, vwarm, nelem_fluid, N, False, args.n, pr)}
+        vctx.close()
+        return out
+
+    # the aggregation-multigrid preconditioner (extension): FP64, same stopping test
+    mgk = fp64_variant(multigrid=True) if args.precision in ("both", "fp64") else None
+
     # the two-level preconditioner (extension): FP64, same stopping test
     two = None
     if args.precision in ("both", "fp64"):
@@ -333,9 +455,12 @@ def arm_gpu(args):
                  "rel_l2_u_vs_fp64": float(np.linalg.norm(um - u0) / np.linalg.norm(u0)),
                  "rel_l2_p_vs_fp64": float(np.linalg.norm(pm - p0) / np.linalg.norm(p0)),
                  "pcg_iterations_per_step": (mst.cg_iterations_total - mwarm.cg_iterations_total) / args.steps,
-                 "roofline": roofline(mst, mwarm, nelem_fluid, N, True, args.n)}
+                 "roofline": roofline(mst, mwarm, nelem_fluid, N, True, args.n, pr)}
         mixed["gpu_launches"] = int(mst.kernel_launches)
         mctx.close()
+
+    hbm = hbm_case(args, local, dist) if args.hbm_n > 0 else None
+    bat = batch_key(args, local, dist) if args.batch_steps > 0 else None
 
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
@@ -353,12 +478,18 @@ def arm_gpu(args):
                              "about 0.6 GB at 64^3",
                        "parallelism": "replicas" if ws > 1 else "single"},
             "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches, "clocks": clk,
-            "pcg_iterations_per_step": its_per_step, "pcg_share_of_step": pcg_share,
+            "pcg_iterations_per_step": its_per_step, "pcg_share_of_step": pcg_share, "probes": pr,
         }
         if mixed is not None:
             line["mixed"] = mixed
+        if mgk is not None:
+            line["multigrid"] = mgk
         if two is not None:
             line["two_level"] = two
+        if hbm is not None:
+            line["hbm_case"] = hbm
+        if bat is not None:
+            line["batch"] = bat
         print(json.dumps(line))
     if dist is not None:
         barrier(dist)

@@ -80,7 +80,7 @@ class Mesh(ctypes.Structure):
 class Options(ctypes.Structure):
     _fields_ = [("precision", _i), ("device", _i), ("inner_tol", _d), ("use_graph", _i),
                 ("pcg_blocks", _i), ("verbose", _i), ("time_pcg", _i), ("pcg_kernel", _i), ("case_cache", _i),
-                ("pcg_two_level", _i)]
+                ("pcg_two_level", _i), ("pcg_multigrid", _i)]
 
 
 class CGResult(ctypes.Structure):
@@ -283,7 +283,8 @@ class Context:
 
     def __init__(self, case=None, case_name: str | None = None, precision: int = FP64, device: int = 0,
                  inner_tol: float = 0.05, use_graph: bool = True, pcg_blocks: int = 0, time_pcg: bool = False,
-                 pcg_kernel: int = 0, case_cache: bool = False, two_level: bool = False):
+                 pcg_kernel: int = 0, case_cache: bool = False, two_level: bool = False,
+                 multigrid: bool = False):
         L = lib()
         self.h = ctypes.c_void_p()
         self.device = device
@@ -291,6 +292,7 @@ class Context:
         opt = make_options(precision, device, inner_tol, use_graph, pcg_blocks, time_pcg, pcg_kernel)
         opt.case_cache = 1 if case_cache else 0
         opt.pcg_two_level = 1 if two_level else 0
+        opt.pcg_multigrid = 1 if multigrid else 0
         if case_name is not None:
             rc = L.cbs3d_create_from_case(case_name.encode(), ctypes.byref(opt), ctypes.byref(self.h), err, 1024)
         else:
@@ -472,7 +474,7 @@ class PressureSolver:
     """Drop-in for ConjugateGradient::solvePressure on the GPU."""
 
     def __init__(self, intma, mat_elem, bc_list, bc_values, precision: int = FP64, device: int = 0,
-                 inner_tol: float = 0.05):
+                 inner_tol: float = 0.05, multigrid: bool = False):
         L = lib()
         self.h = ctypes.c_void_p()
         intma = np.ascontiguousarray(intma, dtype=np.int32).reshape(-1)
@@ -483,6 +485,7 @@ class PressureSolver:
         self.npoin = int(intma.max())
         err = ctypes.create_string_buffer(1024)
         opt = make_options(precision, device, inner_tol)
+        opt.pcg_multigrid = 1 if multigrid else 0
         rc = L.cbs3d_pcg_create(self.nelem, self.npoin, _ptr(intma), _ptr(mat), bl.size, _ptr(bl), _ptr(bv),
                                 ctypes.byref(opt), ctypes.byref(self.h), err, 1024)
         if rc != 0:

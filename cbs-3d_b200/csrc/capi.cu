@@ -176,7 +176,7 @@ void cbs3d_ctx::setup(bool own_pcg)
     S.elcoe2p = buf.alloc<double>(N);
     S.pdiag = buf.alloc<double>(N);
     S.mdiag_real = buf.alloc<double>(N);
-    S.elbuf = buf.alloc<double>(12 * E);
+    S.elbuf = buf.alloc<double>(16 * E);   // Step 1: 4 records of 4 doubles per tet; others use 12*E
     S.dscal = buf.alloc<double>(32);
     S.dtmin_bits = buf.alloc<unsigned long long>(1);
     S.status = buf.alloc<DevStatus>(1);
@@ -202,7 +202,7 @@ void cbs3d_ctx::setup(bool own_pcg)
     if (!own_pcg) return;
     pcg.inner_tol = opt.inner_tol > 0.0 ? opt.inner_tol : 0.05;
     pcg.init(m, S.nflag, S.pfix, S.status, opt.device, opt.pcg_blocks, opt.precision == CBS3D_MIXED, opt.pcg_kernel,
-             opt.pcg_two_level > 0);
+             opt.pcg_two_level > 0, opt.pcg_multigrid > 0);
 }
 
 void cbs3d_ctx::check_status()
@@ -511,7 +511,7 @@ static DevStatus collect_call(cbs3d_ctx* c, int done, int start, long long launc
     stats->kernel_launches = c->launches - launches0;
     if (!c->batch_out) {
         stats->pcg_bytes_per_iter = static_cast<double>(c->pcg.bytes_per_iter());
-        stats->pcg_kernel = c->pcg.coarse ? 6 : c->pcg.variant == 4 && c->pcg.mixed_ok ? 5 : c->pcg.variant;
+        stats->pcg_kernel = c->pcg.mgh ? 7 : c->pcg.coarse ? 6 : c->pcg.variant == 4 && c->pcg.mixed_ok ? 5 : c->pcg.variant;
     }
     for (int k = 0; k + 1 < c->pcg_ev_used; k += 2) {
         float pm = 0.0f;
@@ -914,7 +914,7 @@ cbs3d_status cbs3d_pcg_create(int nelem, int npoin, const int* intma, const int*
         p->d_pdiag = p->buf.alloc<double>(N);
         p->eng.inner_tol = p->opt.inner_tol > 0.0 ? p->opt.inner_tol : 0.05;
         p->eng.init(m, p->d_nflag, p->d_pfix, p->d_status, p->opt.device, p->opt.pcg_blocks,
-                    p->opt.precision == CBS3D_MIXED, p->opt.pcg_kernel);
+                    p->opt.precision == CBS3D_MIXED, p->opt.pcg_kernel, false, p->opt.pcg_multigrid > 0);
         *out = p.release();
         return CBS3D_OK;
     } catch (const Error& e) {

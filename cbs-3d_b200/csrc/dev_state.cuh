@@ -76,7 +76,9 @@ struct DevState {
     // residual.  Both null when no body force is set.
     const double* bforce;
     const double* mfluid;
-    // element-local scratch (12E doubles, reused by every assembly stage)
+    // element-local scratch (16E doubles, reused by every assembly stage):
+    // Step 1 writes node-major 32-byte records [(4e + a)*4 + d] (d < 3, one
+    // pad), the other stages structure-of-arrays [(d*4 + a)*E + e]
     double* elbuf;
     // scalars
     double* dscal;              // [0] dtreal (as double), [1] rtime, [2..16] hb

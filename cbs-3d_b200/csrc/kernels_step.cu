@@ -4,7 +4,8 @@
 // same association order and is compiled with -fmad=false, so each local
 // contribution is bit-identical to the reference's.  Nodal assembly is
 // atomic-free and deterministic: element kernels write their local vectors
-// to a structure-of-arrays scratch (elbuf), and node kernels gather them
+// to a scratch (elbuf: node-major sector records for Step 1, structure of
+// arrays for the others), and node kernels gather them
 // through incidence lists sorted in the reference's summation order --
 // (colour, element) for the coloured Step-1 scatter, element order for the
 // serial assemblies -- so the nodal sums are bit-identical too.  The node
@@ -589,10 +590,15 @@ __global__ void __launch_bounds__(128) k_step1_elem(DevState S)
         }
     }
 #undef LUNK
+    // node-major records of 32 bytes per (element, local node): the three
+    // components and a zero pad, so a node's gather reads exactly one sector
+    // per incident tet and no sector is shared by two nodes
+    double2* rec = reinterpret_cast<double2*>(S.elbuf) + (size_t)e * 8;
 #pragma unroll
-    for (int i = 0; i < 3; ++i)
-#pragma unroll
-        for (int a = 0; a < 4; ++a) S.elbuf[(size_t)(i * 4 + a) * E + e] = lr[i][a];
+    for (int a = 0; a < 4; ++a) {
+        rec[2 * a] = make_double2(lr[0][a], lr[1][a]);
+        rec[2 * a + 1] = make_double2(lr[2][a], 0.0);
+    }
 }
 
 // Colour-ordered nodal gather of the Step-1 residual, predictor
@@ -602,33 +608,33 @@ __global__ void k_step1_node(DevState S)
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= S.P.N) return;
-    const int E = S.P.E;
     double r0 = 0.0, r1 = 0.0, r2 = 0.0;
-    // colour order, records loaded four at a time
+    // colour order, records (one 32-byte sector per incident tet, see
+    // k_step1_elem) loaded four at a time
+    const double2* rec = reinterpret_cast<const double2*>(S.elbuf);
     const int kb = S.n2c_ptr[i], ke = S.n2c_ptr[i + 1];
     int k = kb;
     for (; k + 4 <= ke; k += 4) {
-        double x0[4], x1[4], x2[4];
+        double2 x01[4], x2[4];
 #pragma unroll
         for (int u = 0; u < 4; ++u) {
-            const int ent = S.n2c[k + u];
-            const int e = ent >> 2, a = ent & 3;
-            x0[u] = S.elbuf[(size_t)(0 * 4 + a) * E + e];
-            x1[u] = S.elbuf[(size_t)(1 * 4 + a) * E + e];
-            x2[u] = S.elbuf[(size_t)(2 * 4 + a) * E + e];
+            const size_t q = 2 * (size_t)S.n2c[k + u];   // ent = 4e + a: the record's first double2
+            x01[u] = rec[q];
+            x2[u] = rec[q + 1];
         }
 #pragma unroll
         for (int u = 0; u < 4; ++u) {
-            r0 += x0[u];
-            r1 += x1[u];
-            r2 += x2[u];
+            r0 += x01[u].x;
+            r1 += x01[u].y;
+            r2 += x2[u].x;
         }
     }
     for (; k < ke; ++k) {
-        const int e = S.n2c[k] >> 2, a = S.n2c[k] & 3;
-        r0 += S.elbuf[(size_t)(0 * 4 + a) * E + e];
-        r1 += S.elbuf[(size_t)(1 * 4 + a) * E + e];
-        r2 += S.elbuf[(size_t)(2 * 4 + a) * E + e];
+        const size_t q = 2 * (size_t)S.n2c[k];
+        const double2 x01 = rec[q], x2 = rec[q + 1];
+        r0 += x01.x;
+        r1 += x01.y;
+        r2 += x2.x;
     }
     if (S.bforce) {
         const double mf = S.mfluid[i];

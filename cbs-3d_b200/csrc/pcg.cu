@@ -20,6 +20,7 @@
 // fixed order, so alpha, beta and the stopping decision are identical in all
 // CTAs and reproducible run to run.
 #include "pcg.cuh"
+#include "mg.cuh"
 
 #include <algorithm>
 #include <cstdio>
@@ -294,15 +295,43 @@ __global__ void __launch_bounds__(PCG_THREADS, PCG_CTAS_PER_SM) k_pcg64(PcgDev D
             const uint8_t f = D.nflag[i];
             const bool freen = (f & 1) && !(f & 4);
             double off = 0.0, pci;
+            // four slots' columns and coefficients are loaded before their
+            // gathers, so each lane keeps more loads in flight (the sum still
+            // runs over the slots in order)
             if (upd) {
-                for (int k = 0; k < w; ++k) {
-                    const int j = D.col[base + 32LL * k];
-                    off = fma(D.val[base + 32LL * k], fma(beta, __ldcg(pp + j), __ldcg(D.z + j)), off);
+                for (int k0 = 0; k0 < w; k0 += 4) {
+                    int c[4];
+                    double v[4];
+#pragma unroll
+                    for (int u = 0; u < 4; ++u) {
+                        c[u] = k0 + u < w ? D.col[base + 32LL * (k0 + u)] : i;
+                        v[u] = k0 + u < w ? D.val[base + 32LL * (k0 + u)] : 0.0;
+                    }
+                    double x[4];
+#pragma unroll
+                    for (int u = 0; u < 4; ++u) x[u] = fma(beta, __ldcg(pp + c[u]), __ldcg(D.z + c[u]));
+#pragma unroll
+                    for (int u = 0; u < 4; ++u)
+                        if (k0 + u < w) off = fma(v[u], x[u], off);
                 }
                 pci = freen ? fma(beta, pp[i], D.z[i]) : 0.0;
                 pc[i] = pci;
             } else {
-                for (int k = 0; k < w; ++k) off = fma(D.val[base + 32LL * k], __ldcg(pc + D.col[base + 32LL * k]), off);
+                for (int k0 = 0; k0 < w; k0 += 4) {
+                    int c[4];
+                    double v[4];
+#pragma unroll
+                    for (int u = 0; u < 4; ++u) {
+                        c[u] = k0 + u < w ? D.col[base + 32LL * (k0 + u)] : i;
+                        v[u] = k0 + u < w ? D.val[base + 32LL * (k0 + u)] : 0.0;
+                    }
+                    double x[4];
+#pragma unroll
+                    for (int u = 0; u < 4; ++u) x[u] = __ldcg(pc + c[u]);
+#pragma unroll
+                    for (int u = 0; u < 4; ++u)
+                        if (k0 + u < w) off = fma(v[u], x[u], off);
+                }
                 pci = pc[i];
             }
             const double qi = freen ? fma(D.pdiag[i], pci, off) : 0.0;
@@ -2013,6 +2042,65 @@ cbs3d_status selftest_wait_timeout(int device, int* observed)
     return CBS3D_OK;
 }
 
+namespace {
+// Back-to-back grid all-reduces of the single-reduction kernel's kind (five
+// values per CTA, 512-thread CTAs, one per SM), each depending on the last.
+__global__ void __launch_bounds__(512, 1) k_allreduce_probe(PcgDev D, int iters, double* out)
+{
+    const SegView g = seg_view<false>(D);
+    Acc6 t{0.0, 0.0, 0.0, 0.0, 0.0};
+    for (int i = 0; i < iters; ++i) {
+        Acc6 v{1.0 + t.a * 1.0e-300, (double)blockIdx.x, 0.0, 0.0, (double)threadIdx.x};
+        if (!grid_allreduce3<512>(v, D, g, i, t)) return;
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) out[0] = t.a;
+}
+}  // namespace
+
+cbs3d_status allreduce_probe(int device, int iters, double* us)
+{
+    if (iters < 1 || !us) return CBS3D_INVALID_INPUT;
+    CUDA_OK(cudaSetDevice(device));
+    int sms = 0;
+    CUDA_OK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
+    int per = 0;
+    CUDA_OK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_allreduce_probe, 512, 0));
+    if (per < 1) return CBS3D_CUDA_ERROR;
+    PcgDev D{};
+    D.nslices = sms;
+    D.part = dalloc<double>(static_cast<size_t>(sms) * 16);
+    D.bar = dalloc<unsigned>(4);
+    D.status = dalloc<DevStatus>(1);
+    double* out = dalloc<double>(1);
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    cbs3d_status rc = CBS3D_OK;
+    float ms = 0.0f;
+    CUDA_OK(cudaEventCreate(&e0));
+    CUDA_OK(cudaEventCreate(&e1));
+    for (int rep = 0; rep < 2 && rc == CBS3D_OK; ++rep) {   // the first launch warms up
+        CUDA_OK(cudaMemset(D.bar, 0, 4 * sizeof(unsigned)));
+        CUDA_OK(cudaMemset(D.status, 0, sizeof(DevStatus)));
+        void* args[] = {&D, &iters, &out};
+        CUDA_OK(cudaEventRecord(e0));
+        CUDA_OK(cudaLaunchCooperativeKernel(reinterpret_cast<const void*>(k_allreduce_probe), dim3(sms), dim3(512),
+                                            args, 0, nullptr));
+        CUDA_OK(cudaEventRecord(e1));
+        CUDA_OK(cudaEventSynchronize(e1));
+        CUDA_OK(cudaEventElapsedTime(&ms, e0, e1));
+        DevStatus h{};
+        CUDA_OK(cudaMemcpy(&h, D.status, sizeof h, cudaMemcpyDeviceToHost));
+        if (h.code != 0) rc = static_cast<cbs3d_status>(h.code);
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    cudaFree(D.part);
+    cudaFree(D.bar);
+    cudaFree(D.status);
+    cudaFree(out);
+    if (rc == CBS3D_OK) *us = 1.0e3 * ms / iters;
+    return rc;
+}
+
 cbs3d_status coarse_inverse(int device, int g, const double* a, double* ainv, int variant)
 {
     if (!a || !ainv || g < 1 || (variant != 0 && variant != 1) || g > (variant == 0 ? CINV_MAX : 164))
@@ -2073,6 +2161,19 @@ const void* fn_mixed_single(int rmax, int nt) { return nt == 256 ? fn_mixed<fals
 constexpr int BATCH_THREADS = 256;
 
 }  // namespace
+
+void coarse_invert_launch(int g, double* a, cudaStream_t st)
+{
+    k_coarse_invert_reg<<<1, 512, 0, st>>>(g, a);
+}
+
+cudaError_t pcg_raise_smem_limit(const void* fn, size_t smem) { return raise_smem_limit(fn, smem); }
+
+int PcgEngine::launches_per_solve() const
+{
+    if (mgh) return 4 + mgh->launches_per_setup();
+    return coarse ? 6 : 4;
+}
 
 void PcgEngine::build_coarse(const HostModel& m, const std::vector<int>& colp)
 {
@@ -2170,7 +2271,8 @@ void PcgEngine::build_coarse(const HostModel& m, const std::vector<int>& colp)
 }
 
 void PcgEngine::init(const HostModel& m, const uint8_t* nflag, const double* pfix, DevStatus* status,
-                     int device, int blocks_override, bool mixed_mode, int kernel_choice, bool two_level)
+                     int device, int blocks_override, bool mixed_mode, int kernel_choice, bool two_level,
+                     bool multigrid)
 {
     N = m.N;
     E = m.E;
@@ -2342,6 +2444,23 @@ void PcgEngine::init(const HostModel& m, const uint8_t* nflag, const double* pfi
         }
     }
     if (two_level && variant == 4 && nthreads == 512 && !mixed_ok) build_coarse(m, colp);
+    if (multigrid && !mixed && !coarse) {
+        mgh = new MgHierarchy;
+        bool ok = false;
+        try {
+            ok = mgh->build(m, colp, d_slice_off, d_slice_w, d_col, device, sms, blocks_override);
+        } catch (...) {
+            mgh->release();
+            delete mgh;
+            mgh = nullptr;
+            throw;
+        }
+        if (!ok) {
+            mgh->release();
+            delete mgh;
+            mgh = nullptr;
+        }
+    }
     d_part = dalloc<double>(static_cast<size_t>(nblocks) * 16);
     d_bar = dalloc<unsigned>(4);
     d_out = dalloc<CgOut>(1);
@@ -2366,6 +2485,12 @@ void PcgEngine::init(const HostModel& m, const uint8_t* nflag, const double* pfi
 
 void PcgEngine::release()
 {
+    if (mgh) {
+        mgh->release();
+        delete mgh;
+        mgh = nullptr;
+    }
+    mg_ready = false;
     void* ptrs[] = {d_slice_off, d_slice_w, d_col, d_cptr, d_cent, d_val, d_val32, d_r, d_z, d_pA,
                     d_pB, d_q, d_f32, d_part, d_bar, d_out, d_halo_ptr, d_halo_idx, d_lcol, d_row_node,
                     d_xp, d_bp, d_dp, d_fp, d_pair_ptr, d_pair_ij, d_pair_ent, d_ac, d_nbr_ptr, d_nbr_ids, d_hown};
@@ -2394,6 +2519,11 @@ void PcgEngine::coarse_setup(const double* pdiag, const int* row_node, cudaStrea
 
 void PcgEngine::prepare_coarse(const double* d_pdiag_node, cudaStream_t st)
 {
+    if (mgh) {
+        mgh->setup(d_val, d_pdiag_node, d_row_node, st);
+        mg_ready = true;
+        return;
+    }
     if (!coarse) return;
     coarse_setup(d_pdiag_node, d_row_node, st);
     coarse_ready = true;
@@ -2464,9 +2594,19 @@ cbs3d_status PcgEngine::solve(double* pres, double* rhs1, double* pdiag, int pre
         fn = fn_twolevel(rmax);
         smem = coarse_smem;
     }
-    if (ev0) CUDA_OK(cudaEventRecord(ev0, st));
-    CUDA_OK(cudaLaunchCooperativeKernel(fn, dim3(nblocks), dim3(nthreads), coarse ? args2 : args, smem, st));
-    if (ev1) CUDA_OK(cudaEventRecord(ev1, st));
+    if (mgh && precond == 1) {
+        // the multigrid set-up of this solve, unless prepare_coarse made it
+        if (!mg_ready) mgh->setup(d_val, d_dp, nullptr, st);
+        mg_ready = false;
+        if (ev0) CUDA_OK(cudaEventRecord(ev0, st));
+        mgh->launch(D, st);
+        if (ev1) CUDA_OK(cudaEventRecord(ev1, st));
+    } else {
+        mg_ready = false;
+        if (ev0) CUDA_OK(cudaEventRecord(ev0, st));
+        CUDA_OK(cudaLaunchCooperativeKernel(fn, dim3(nblocks), dim3(nthreads), coarse ? args2 : args, smem, st));
+        if (ev1) CUDA_OK(cudaEventRecord(ev1, st));
+    }
     k_perm_out<<<(NP + 255) / 256, 256, 0, st>>>(D, d_xp, pres);
     if (sync) CUDA_OK(cudaStreamSynchronize(st));
     return CBS3D_OK;
@@ -2491,6 +2631,16 @@ cbs3d_status PcgEngine::read_result(cbs3d_cg_result& r, cudaStream_t st)
 
 size_t PcgEngine::bytes_per_iter() const
 {
+    if (mgh) {
+        // level 0: three products (pre-smoothing residual, post-smoothing,
+        // A p) over the coefficients; per node the pressure read and written,
+        // z and q written and read back, the smoothed residual written and
+        // read by the restriction; coarse levels: two products each
+        size_t b = static_cast<size_t>(nnz_offdiag) * 24 + static_cast<size_t>(N) * 64;
+        for (int l = 1; l < mgh->Lc; ++l)
+            b += static_cast<size_t>(mgh->n[static_cast<size_t>(l)]) * (16 * mgh->W[static_cast<size_t>(l)] + 48);
+        return b;
+    }
     if (variant == 4 && mixed_ok) {
         // coefficients resident in shared memory; per node: r, w, s of the
         // previous iteration read once for staging (12), r, s, w written (12),

@@ -68,6 +68,8 @@ struct PcgDev {
                                  // and diagonal (2*RMAX*threads doubles); 0: read from global memory
 };
 
+class MgHierarchy;
+
 // Two-level preconditioner data of one launch: the coarse space is one
 // aggregate per CTA (its free rows); ainv is the inverse of the aggregated
 // operator P^T A P, nbr_ptr/nbr_ids each CTA's own and halo-owner CTAs, and
@@ -89,8 +91,11 @@ public:
     // 4 as 3 with one grid synchronisation per iteration (Chronopoulos-Gear)
     // two_level: Jacobi plus a coarse correction on one aggregate per CTA
     // (large meshes with the single-reduction kernel; else plain Jacobi)
+    // multigrid: the aggregation-multigrid preconditioned CG (mg.cuh) for
+    // Jacobi-preconditioned FP64 solves, where the mesh fits it
     void init(const HostModel& m, const uint8_t* d_nflag, const double* d_pfix, DevStatus* d_status,
-              int device, int blocks_override, bool mixed, int kernel_choice = 0, bool two_level = false);
+              int device, int blocks_override, bool mixed, int kernel_choice = 0, bool two_level = false,
+              bool multigrid = false);
     void release();
     // ELL values from gstifE*delte (step path) or from a caller's gstif[6E].
     void assemble_from_state(const DevState& S, cudaStream_t st);
@@ -104,13 +109,15 @@ public:
     cbs3d_status solve(double* d_pres, double* d_rhs1, double* d_pdiag, int precond, int conv_test,
                        int max_iter, double rel_tol, double abs_tol, cudaStream_t st, bool sync,
                        cudaEvent_t ev0 = nullptr, cudaEvent_t ev1 = nullptr);
-    // impose, permute in, solver, permute out
-    int launches_per_solve() const { return coarse ? 6 : 4; }
+    // impose, permute in, solver, permute out (+ the preconditioner's set-up)
+    int launches_per_solve() const;
     cbs3d_status read_result(cbs3d_cg_result& r, cudaStream_t st);
     // y = A x with the assembled operator (identity rows on fixed nodes).
     void multiply(const double* d_pdiag, const double* d_x, double* d_y, cudaStream_t st);
 
     bool mixed = false;
+    MgHierarchy* mgh = nullptr;  // multigrid in use (else null)
+    bool mg_ready = false;       // prepare_coarse set the multigrid up for the next solve
     int rmax = 0;            // rows per thread of the register-resident kernels (0: global kernel)
     int nthreads = 512;      // CTA size of the persistent kernel
     bool coarse = false;     // two-level preconditioner in use
@@ -238,6 +245,10 @@ private:
     CgOut* d_out = nullptr;
     PcgDev base{};
 };
+
+// Microseconds per grid all-reduce of the single-reduction kernel (one
+// 512-thread CTA per SM, `iters` back-to-back all-reduces, CUDA events).
+cbs3d_status allreduce_probe(int device, int iters, double* us);
 
 // Launches a grid whose barrier can never complete and reports the status
 // the bounded waits recorded (CBS3D_TIMEOUT when they ran out as designed).

@@ -103,6 +103,12 @@ typedef struct cbs3d_options {
     int pcg_two_level;       /* extension: Jacobi plus a coarse correction on one aggregate of rows
                                 per CTA (the aggregated operator is rebuilt and inverted every solve);
                                 same stopping test, far fewer iterations; large meshes only */
+    int pcg_multigrid;       /* extension (the counterpart of the reference's PETSc/AMG path,
+                                src/linalg/PetscPressureSolver.cpp:335-360): aggregation-multigrid
+                                V-cycle preconditioned CG in place of Jacobi-PCG; hierarchy fixed by
+                                the mesh (aggregates of 8 Morton-ordered rows), Galerkin coarse
+                                operators rebuilt every solve, same stopping test; FP64, for meshes
+                                up to 655,360 row positions (else Jacobi) */
 } cbs3d_options;
 
 /* Mirrors ConjugateGradient::Result (include/cbs/linalg/ConjugateGradient.hpp:36-68).
@@ -135,7 +141,8 @@ typedef struct cbs3d_step_stats {
     double pcg_bytes_per_iter; /* bytes one PCG iteration of the selected kernel moves */
     int pcg_kernel;          /* PCG kernel in use: 1 global vectors, 2 register rows,
                                 3 shared-memory halo, 4 single-reduction (CG-CG),
-                                5 mixed FP32/FP64, 6 two-level (CG-CG + coarse correction) */
+                                5 mixed FP32/FP64, 6 two-level (CG-CG + coarse correction),
+                                7 aggregation-multigrid preconditioned CG */
 } cbs3d_step_stats;
 
 typedef struct cbs3d_ctx cbs3d_ctx;
@@ -388,6 +395,19 @@ cbs3d_status cbs3d_selftest_wait_timeout(int device, int* observed_status);
  * zero diagonal entry is replaced by 1 first, as for an empty aggregate.
  * a and ainv are host arrays of g*g doubles. */
 cbs3d_status cbs3d_coarse_inverse(int device, int g, const double* a, double* ainv, int variant);
+
+/* Measurement probes (no reference counterpart) that the benchmark uses to
+ * state the solver kernels' rooflines.  cbs3d_probe_copy_bandwidth: GB/s of
+ * a copy between two device buffers of `bytes` each (read + write bytes over
+ * the CUDA-event time of `reps` launches after three warm-up launches): a
+ * pair that fits in L2 gives the L2 copy bandwidth, a larger one the HBM copy
+ * bandwidth.  cbs3d_probe_allreduce: microseconds per grid-wide all-reduce
+ * of the persistent PCG kernel's kind (one 512-thread CTA per SM, five
+ * values, `iters` dependent all-reduces in one cooperative launch) -- the
+ * per-iteration latency floor of the single-reduction PCG.  Both allocate
+ * and free their own device memory. */
+cbs3d_status cbs3d_probe_copy_bandwidth(int device, long long bytes, int reps, double* gbs);
+cbs3d_status cbs3d_probe_allreduce(int device, int iters, double* us_per_allreduce);
 
 #ifdef __cplusplus
 }

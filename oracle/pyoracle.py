@@ -16,6 +16,8 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "_build", "libcbs_oracle.so")
 REF_HARNESS = os.path.join(HERE, "_ref", "cbs_ref_harness")
+# the same harness with Step 2's pressure solve on the GPU drop-in (cbs3d_pcg_solve)
+REF_GPU_HARNESS = os.path.join(HERE, "_ref", "cbs_ref_gpu_harness")
 
 
 class OrcParams(ctypes.Structure):
@@ -185,9 +187,9 @@ def read_dump(directory: str) -> dict:
 
 
 def run_reference(case_base: str, nsteps: int, outdir: str, stage: int = 0, every: int = 0,
-                  threads: int = 1) -> dict:
+                  threads: int = 1, gpu_pressure: bool = False) -> dict:
     os.makedirs(outdir, exist_ok=True)
-    cmd = [REF_HARNESS, case_base, str(nsteps), outdir]
+    cmd = [REF_GPU_HARNESS if gpu_pressure else REF_HARNESS, case_base, str(nsteps), outdir]
     if stage:
         cmd += ["--stage", str(stage)]
     if every:

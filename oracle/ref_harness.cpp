@@ -7,6 +7,11 @@
 // It writes raw little-endian arrays for the golden fixtures and times the
 // step loop for the CPU baseline.  Nothing in the product links this file.
 //
+// Built with -DCBS_GPU_PRESSURE (cbs_ref_gpu_harness) the pressure solve of
+// Step 2 goes through the GPU backend of gpu_pressure_solver.inc -- the
+// INTEGRATION.md adapter calling cbs3d_pcg_solve -- instead of
+// ConjugateGradient::solvePressure; everything else stays the reference's.
+//
 // usage:
 //   cbs_ref_harness <case> <nsteps> <outdir> [--stage K] [--every M] [--time]
 //     --stage K   dump every intermediate array of step K (1-based)
@@ -43,6 +48,10 @@
 #include <vector>
 
 using namespace cbs;
+
+#ifdef CBS_GPU_PRESSURE
+#include "gpu_pressure_solver.inc"
+#endif
 
 namespace
 {
@@ -181,7 +190,11 @@ namespace
             MatrixVectorCalc::pressureMultiply(s, s.pres, y);
             dump("s4_Apres", y);
         }
+#ifdef CBS_GPU_PRESSURE
+        ConjugateGradient::Result r = GpuPressureSolver::solvePressure(s);
+#else
         ConjugateGradient::Result r = ConjugateGradient::solvePressure(s);
+#endif
         s.last_cg_iterations = r.iterations;
         s.last_cg_initial_l2 = r.initial_l2;
         s.last_cg_final_l2 = r.final_l2;

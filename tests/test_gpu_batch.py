@@ -148,3 +148,28 @@ def test_engines_of_different_sizes_coexist():
     bs = gpu.Batch(_uneven(count=2, seed=2), autotune=False, rows_per_thread=8)
     bb.step(2)
     bs.step(2)
+
+
+def test_gpu_runner_drives_the_batch_on_one_device():
+    """cbs3d.batch.run_sharded with the real gpu_runner on one GPU: every
+    instance steps, and splitting the instances into the two LPT shards of a
+    two-rank run (each shard its own batch, run one after the other here)
+    gives every instance the PCG iteration counts of the single batch to
+    within 2 (the CTAs an instance gets, and so its reduction order, depend on
+    the batch it is packed with)."""
+    from cbs3d import cases
+    from cbs3d.batch import gpu_runner, lpt_shard, run_sharded
+    cs = cases.cavity_batch(count=8, n_lo=4, n_hi=12)
+    runner = gpu_runner(device=0)
+    whole = run_sharded(cs, 3, 0, 1, runner)
+    assert [m["instance"] for m in whole] == list(range(len(cs)))
+    assert all(m["steps"] == 3 and m["cg_iterations"] > 0 for m in whole)
+    shards = lpt_shard([c.mesh.nelem for c in cs], 2)
+    assert all(shards)
+    split = {}
+    for part in shards:
+        for i, m in zip(part, runner([cs[i] for i in part], 3)):
+            split[i] = m
+    for m in whole:
+        assert abs(split[m["instance"]]["cg_iterations"] - m["cg_iterations"]) <= 2
+        assert split[m["instance"]]["nelem"] == m["nelem"]

@@ -1,8 +1,14 @@
 """The benchmark configurations at full mesh size against the reference run
-on them (tests/golden/make_config_golden.py): 64^3 jittered cavity
-(1,572,864 tets), 96x16x16 channel (147,456 tets) and the conjugate-heat-
-transfer slab (552,960 tets), three steps each.  Time steps are bitwise; the
-fields agree to RUN_TOL relative L2 at 4,000 seeded nodes and in norm."""
+on them for their stated step counts (tests/golden/make_config_golden.py):
+64^3 jittered cavity (1,572,864 tets) for 200 steps, 96x16x16 channel
+(147,456 tets) for 200 and the conjugate-heat-transfer slab (552,960 tets)
+for 300.  The FP64 Jacobi engine -- the drop-in for the reference's
+native-PCG path -- agrees with the reference to RUN_TOL relative L2 on u, p
+and T at 4,000 seeded nodes and in norm, after every 50th step and at the
+end; its time steps agree bitwise over the first steps and to DT_TOL later,
+its PCG iteration counts to within 3.  The two-level and multigrid
+preconditioners (extensions: same stopping test, other iterates) are held to
+EXT_TOL over the same runs."""
 import json
 import os
 import sys
@@ -14,8 +20,11 @@ from helpers import rel_l2
 
 pytestmark = pytest.mark.gpu
 
-RUN_TOL = 1e-8
+RUN_TOL = 1e-10
+EXT_TOL = 1e-8
+DT_TOL = 1e-10
 HERE = os.path.dirname(os.path.abspath(__file__))
+NAMES = ["cfg2_cavity64", "cfg4_channel", "cfg5_cht"]
 
 
 def _load(name):
@@ -28,27 +37,46 @@ def _load(name):
     return case, z
 
 
-@pytest.mark.parametrize("two_level", [False, True])
-@pytest.mark.parametrize("name", ["cfg2_cavity64", "cfg4_channel", "cfg5_cht"])
-def test_config_full_size_vs_reference(name, two_level):
-    """Jacobi (the reference's preconditioner) and the two-level extension,
-    which takes fewer iterations to the same stopping test."""
+def _check_fields(case, z, u, p, t, key, tol):
+    """Sampled fields and whole-field norms of one snapshot ('' = final)."""
+    idx = z["idx"]
+    if key:
+        ru, rp, norms = z[f"snap{key}_u"], z[f"snap{key}_p"], z[f"snap{key}_norms"]
+        rt = z[f"snap{key}_t"] if f"snap{key}_t" in z else None
+    else:
+        ru, rp = z["u"], z["p"]
+        norms = np.array([z["norm_u"][0], z["norm_p"][0], z["norm_t"][0]])
+        rt = z["t"]
+    errs = {"u": rel_l2(u.reshape(-1, 3)[idx], ru), "p": rel_l2(p[idx], rp),
+            "|u|": abs(np.linalg.norm(u) - norms[0]) / norms[0], "|p|": abs(np.linalg.norm(p) - norms[1]) / norms[1]}
+    if case.params.get("temp_calc", 0):
+        errs["t"] = rel_l2(t[idx], rt)
+        errs["|t|"] = abs(np.linalg.norm(t) - norms[2]) / norms[2]
+    print(f"step {key or 'final'}: " + " ".join(f"{k} {v:.2e}" for k, v in errs.items()))
+    for k, v in errs.items():
+        assert v <= tol, (key, k, v)
+
+
+@pytest.mark.parametrize("mode", ["jacobi", "two_level", "multigrid"])
+@pytest.mark.parametrize("name", NAMES)
+def test_config_full_size_vs_reference(name, mode):
     from cbs3d import gpu
     case, z = _load(name)
     n = int(z["nsteps"][0])
     hist = z["history"].reshape(n, 21)
-    ctx = gpu.Context(case, two_level=two_level)
-    for s in range(n):
+    snaps = {int(k) for k in z["snap_steps"]}
+    ctx = gpu.Context(case, two_level=mode == "two_level", multigrid=mode == "multigrid")
+    tol = RUN_TOL if mode == "jacobi" else EXT_TOL
+    for s in range(1, n + 1):
         st = ctx.step(1)
-        assert st.dtreal == hist[s, 0]
-        if not two_level:
-            assert abs(st.cg.iterations - int(hist[s, 1])) <= 3
+        if mode == "jacobi":
+            if s <= 3:
+                assert st.dtreal == hist[s - 1, 0]
+            else:
+                assert abs(st.dtreal - hist[s - 1, 0]) <= DT_TOL * hist[s - 1, 0]
+            assert abs(st.cg.iterations - int(hist[s - 1, 1])) <= 3, s
+        if s in snaps:
+            u, p, t = ctx.fields()
+            _check_fields(case, z, u, p, t, s, tol)
     u, p, t = ctx.fields()
-    idx = z["idx"]
-    assert rel_l2(u.reshape(-1, 3)[idx], z["u"]) <= RUN_TOL
-    assert rel_l2(p[idx], z["p"]) <= RUN_TOL
-    assert abs(np.linalg.norm(u) - z["norm_u"][0]) <= RUN_TOL * z["norm_u"][0]
-    assert abs(np.linalg.norm(p) - z["norm_p"][0]) <= RUN_TOL * z["norm_p"][0]
-    if case.params.get("temp_calc", 0):
-        assert rel_l2(t[idx], z["t"]) <= RUN_TOL
-        assert abs(np.linalg.norm(t) - z["norm_t"][0]) <= RUN_TOL * z["norm_t"][0]
+    _check_fields(case, z, u, p, t, "", tol)

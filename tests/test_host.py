@@ -239,3 +239,14 @@ def test_bench_reference_arm_contract():
     assert d["impl"] == "reference" and d["value"] > 0 and d["unit"] == "steps/s"
     assert d["cpu_baseline"]["kind"] == "reference" and d["cpu_baseline"]["cores"] >= 1
     assert d["e2e"]["h2d_bytes_per_step"] == 0 and d["e2e"]["value"] == d["value"]
+
+
+def test_integration_snippet_is_the_compiled_backend():
+    """The solver_opt backend shown in INTEGRATION.md is the code that
+    oracle/gpu_pressure_solver.inc compiles into the reference harness."""
+    import re
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    doc = open(os.path.join(root, "INTEGRATION.md")).read()
+    block = re.search(r"```cpp\n(.*?)```", doc, re.S).group(1)
+    inc = open(os.path.join(root, "oracle", "gpu_pressure_solver.inc")).read()
+    assert block.strip() in inc
