@@ -23,7 +23,7 @@ constexpr double MG_GERSH = 1.8;           // weight bound: omega * gershgorin <
 
 // threads per row of coarse level l in the solver kernel (fixed per level,
 // so every row's sum has the same order for any grid size)
-inline int level_tpr(int l) { return l == 1 ? 1 : l == 2 ? 8 : 32; }
+inline int level_tpr(int l) { return l == 1 ? 2 : l == 2 ? 8 : 32; }
 
 __device__ __forceinline__ double smoother_weight(double d, double offabs)
 {
@@ -77,9 +77,11 @@ __global__ void k_mg_weights(const double* val, const int* col, int n, int W, do
     const int I = blockIdx.x * blockDim.x + threadIdx.x;
     if (I >= n) return;
     double a = 0.0;
-    for (int k = 0; k < W; ++k)
-        if (col[(size_t)I * W + k] >= 0) a += fabs(val[(size_t)I * W + k]);
-    wd[I] = smoother_weight(val[(size_t)n * W + I], a);
+    for (int k = 0; k < W; ++k) {
+        const long long s = mg_slot(I, k, W);
+        if (col[s] >= 0) a += fabs(val[s]);
+    }
+    wd[I] = smoother_weight(val[mg_slots(n, W) + I], a);
 }
 
 // The coarsest operator as a dense matrix (rows without free children are
@@ -90,10 +92,10 @@ __global__ void k_mg_dense(const double* val, const int* col, int n, int W, doub
     if (I >= n) return;
     double* row = a + (size_t)I * n;
     for (int J = 0; J < n; ++J) row[J] = 0.0;
-    row[I] = val[(size_t)n * W + I];
+    row[I] = val[mg_slots(n, W) + I];
     for (int k = 0; k < W; ++k) {
-        const int J = col[(size_t)I * W + k];
-        if (J >= 0) row[J] = val[(size_t)I * W + k];
+        const long long s = mg_slot(I, k, W);
+        if (col[s] >= 0) row[col[s]] = val[s];
     }
 }
 
@@ -120,6 +122,35 @@ __device__ __forceinline__ bool mg_arrive_wait(unsigned long long* cnt, unsigned
     return ld_relaxed_int(&st->code) == 0;
 }
 
+// Off-diagonal product of coarse row I over the staged halo values vl: the
+// row's T threads (sub = 0..T-1) take entries sub, sub+T, ... in order, four
+// loads issued at a time, then a fixed xor tree over the T lanes.  All lanes
+// of the warp call it (active false: contributes nothing).
+__device__ __forceinline__ double coarse_row(const MgLevelDev& Lv, int I, int sub, int T, bool active,
+                                             const double* vl)
+{
+    double acc = 0.0;
+    if (active) {
+        const int W = Lv.W;
+        for (int k0 = sub; k0 < W; k0 += 4 * T) {
+            unsigned short lc[4];
+            double v[4];
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                const int k = k0 + u * T;
+                const long long s = mg_slot(I, k < W ? k : 0, W);
+                lc[u] = k < W ? __ldg(Lv.lcol + s) : (unsigned short)0xffffu;
+                v[u] = k < W ? __ldg(Lv.val + s) : 0.0;
+            }
+#pragma unroll
+            for (int u = 0; u < 4; ++u)
+                if (lc[u] != 0xffffu) acc = fma(v[u], vl[lc[u]], acc);
+        }
+    }
+    for (int m = 1; m < T; m <<= 1) acc += __shfl_xor_sync(0xffffffffu, acc, m);
+    return acc;
+}
+
 // ------------------------------------------------------------ solver kernel
 template <int RMAX>
 __global__ void __launch_bounds__(MG_NT, 1) k_pcg_mg(PcgDev D, MgDev M)
@@ -143,8 +174,7 @@ __global__ void __launch_bounds__(MG_NT, 1) k_pcg_mg(PcgDev D, MgDev M)
     DevStatus* status = D.status;
 
     double* rh = reinterpret_cast<double*>(smem_raw);   // halo: CG residual
-    double* wdh = rh + HM;                              // halo: smoother weight / diagonal
-    double* ph = wdh + HM;                              // halo: search direction
+    double* ph = rh + HM;                               // halo: search direction
     double* vh = ph + HM;                               // halo: values the next product reads
     double* dbase = reinterpret_cast<double*>(smem_raw);
     int* ibase = reinterpret_cast<int*>(dbase + M.sd_xc + 2 * M.nc);
@@ -242,17 +272,22 @@ __global__ void __launch_bounds__(MG_NT, 1) k_pcg_mg(PcgDev D, MgDev M)
         r[k] = p[k] = z[k] = dg[k] = wd[k] = 0.0;
         fr[k] = false;
     }
-    // off[k] = sum_j A_ij src[j] over the own rows' off-diagonal slots
-    auto offdiag = [&](const double* src, double* off) {
+    // off[k] = sum_j A_ij src[j] over the own rows' off-diagonal slots, from
+    // the FP64 coefficients or (the cycle's smoothing products, when the
+    // engine keeps them) their FP32 copies
+    auto offdiag = [&](const double* src, double* off, bool fp32 = false) {
 #pragma unroll
         for (int k = 0; k < RMAX; ++k) off[k] = 0.0;
+        const bool f32 = fp32 && D.val32 != nullptr;
         for (int k0 = 0; k0 < wmax; k0 += 2) {
             double v[RMAX][2];
 #pragma unroll
             for (int k = 0; k < RMAX; ++k)
 #pragma unroll
-                for (int u = 0; u < 2; ++u)
-                    v[k][u] = (k0 + u < wr[k]) ? __ldcg(D.val + S0 + lbase[k] + 32 * (k0 + u)) : 0.0;
+                for (int u = 0; u < 2; ++u) {
+                    const long long t = S0 + lbase[k] + 32 * (k0 + u);
+                    v[k][u] = (k0 + u < wr[k]) ? (f32 ? (double)__ldcg(D.val32 + t) : __ldcg(D.val + t)) : 0.0;
+                }
 #pragma unroll
             for (int k = 0; k < RMAX; ++k)
 #pragma unroll
@@ -268,9 +303,10 @@ __global__ void __launch_bounds__(MG_NT, 1) k_pcg_mg(PcgDev D, MgDev M)
     auto vcycle = [&]() -> bool {
         double off[RMAX];
         // level 0: pre-smoothing from zero (x = W r, halo included), residual
-        for (int k = threadIdx.x; k < nh; k += MG_NT) vh[k] = wdh[k] * rh[k];
+        // (the halo's smoother weights are read through L1: constant per solve)
+        for (int k = threadIdx.x; k < nh; k += MG_NT) vh[k] = __ldg(M.wd0 + hidx[k]) * rh[k];
         __syncthreads();
-        offdiag(vh, off);
+        offdiag(vh, off, true);
 #pragma unroll
         for (int k = 0; k < RMAX; ++k) {
             const int i = row[k];
@@ -310,17 +346,11 @@ __global__ void __launch_bounds__(MG_NT, 1) k_pcg_mg(PcgDev D, MgDev M)
             for (int rb = 0; rb < e - o; rb += MG_NT / T) {
                 const int ri = rb + threadIdx.x / T;
                 const int I = o + ri;
-                double acc = 0.0;
-                if (ri < e - o)
-                    for (int k = sub; k < W; k += T) {
-                        const unsigned short lc = __ldg(Lv.lcol + (size_t)I * W + k);
-                        if (lc != 0xffffu) acc = fma(__ldg(Lv.val + (size_t)I * W + k), vl[lc], acc);
-                    }
-                for (int m = 1; m < T; m <<= 1) acc += __shfl_xor_sync(0xffffffffu, acc, m);
+                const double acc = coarse_row(Lv, I, sub, T, ri < e - o, vl);
                 if (ri < e - o && sub == 0) {
                     const int hI = hown + ri;
                     const double w = wl[hI];
-                    const double rho = w > 0.0 ? rl[hI] - __ldg(Lv.val + (size_t)Lv.n * W + I) * vl[hI] - acc : 0.0;
+                    const double rho = w > 0.0 ? rl[hI] - __ldg(Lv.val + mg_slots(Lv.n, W) + I) * vl[hI] - acc : 0.0;
                     __stcg(Lv.rho + I, rho);
                 }
             }
@@ -370,19 +400,13 @@ __global__ void __launch_bounds__(MG_NT, 1) k_pcg_mg(PcgDev D, MgDev M)
             for (int rb = 0; rb < e - o; rb += MG_NT / T) {
                 const int ri = rb + threadIdx.x / T;
                 const int I = o + ri;
-                double acc = 0.0;
-                if (ri < e - o)
-                    for (int k = sub; k < W; k += T) {
-                        const unsigned short lc = __ldg(Lv.lcol + (size_t)I * W + k);
-                        if (lc != 0xffffu) acc = fma(__ldg(Lv.val + (size_t)I * W + k), vl[lc], acc);
-                    }
-                for (int m = 1; m < T; m <<= 1) acc += __shfl_xor_sync(0xffffffffu, acc, m);
+                const double acc = coarse_row(Lv, I, sub, T, ri < e - o, vl);
                 if (ri < e - o && sub == 0) {
                     const int hI = hown + ri;
                     const double w = wl[hI];
                     const double xv = vl[hI];
                     const double xn =
-                        w > 0.0 ? xv + w * (rl[hI] - __ldg(Lv.val + (size_t)Lv.n * W + I) * xv - acc) : 0.0;
+                        w > 0.0 ? xv + w * (rl[hI] - __ldg(Lv.val + mg_slots(Lv.n, W) + I) * xv - acc) : 0.0;
                     __stcg(Lv.x + I, xn);
                 }
             }
@@ -392,12 +416,12 @@ __global__ void __launch_bounds__(MG_NT, 1) k_pcg_mg(PcgDev D, MgDev M)
         const double* x1 = M.Lc > 1 ? M.lv[1].x : nullptr;
         for (int k = threadIdx.x; k < nh; k += MG_NT) {
             const int pos = hidx[k];
-            const double w = wdh[k];
+            const double w = __ldg(M.wd0 + pos);
             const double xcg = x1 ? __ldcg(x1 + (pos >> 3)) : xc[pos >> 3];
             vh[k] = w > 0.0 ? fma(w, rh[k], MG_OVER * xcg) : 0.0;
         }
         __syncthreads();
-        offdiag(vh, off);
+        offdiag(vh, off, true);
 #pragma unroll
         for (int k = 0; k < RMAX; ++k) {
             const int i = row[k];
@@ -432,7 +456,6 @@ __global__ void __launch_bounds__(MG_NT, 1) k_pcg_mg(PcgDev D, MgDev M)
     // ---- r0 = b - A x0 with the reference's constraints and checks
     for (int k = threadIdx.x; k < nh; k += MG_NT) {
         vh[k] = __ldcg(D.pres + hidx[k]);
-        wdh[k] = __ldg(M.wd0 + hidx[k]);
         ph[k] = 0.0;
     }
     __syncthreads();
@@ -591,8 +614,9 @@ T* MgHierarchy::zeros(size_t count)
     return p;
 }
 
-bool MgHierarchy::build(const HostModel& m, const std::vector<int>& colp, const long long* slice_off_d,
-                        const int* slice_w_d, const int* colp_d, int device, int sms, int blocks_override)
+bool MgHierarchy::build(const HostModel& m, const std::vector<int>& colp, const uint8_t* d_nflag,
+                        const long long* slice_off_d, const int* slice_w_d, const int* colp_d, int device, int sms,
+                        int blocks_override)
 {
     (void)device;
     const PressurePattern& P = m.pat;
@@ -605,18 +629,25 @@ bool MgHierarchy::build(const HostModel& m, const std::vector<int>& colp, const 
     // ---- level sizes
     n.assign(1, NP);
     while (n.back() > MG_COARSE_MAX && static_cast<int>(n.size()) <= MG_MAX_LEVELS) n.push_back((n.back() + 7) / 8);
-    if (n.back() > MG_COARSE_MAX || n.size() < 2) return false;
+    if (n.back() > MG_COARSE_MAX || n.size() < 2) {
+        why = n.size() < 2 ? "mesh too small for a hierarchy (at most 160 rows)"
+                           : "more than 8 levels needed for a coarsest level of at most 160 rows";
+        return false;
+    }
     Lc = static_cast<int>(n.size()) - 1;
 
     // ---- partition: chunks of 4 slices, contiguous chunk ranges per CTA
     nchunks = (nslices + MG_CHUNK_SLICES - 1) / MG_CHUNK_SLICES;
     G = std::min(sms, nchunks);
     if (blocks_override > 0) G = std::min(G, blocks_override);
-    if (G < 1) return false;
+    if (G < 1) { why = "empty grid"; return false; }
     const int cpc = (nchunks + G - 1) / G;
     const int per_warp = (cpc * MG_CHUNK_SLICES + MG_NW - 1) / MG_NW;
     rmax = per_warp <= 1 ? 1 : per_warp <= 2 ? 2 : per_warp <= 4 ? 4 : per_warp <= 8 ? 8 : 0;
-    if (!rmax) return false;
+    if (!rmax) {
+        why = "more than 8 slices per warp: the rows do not fit the register tiling";
+        return false;
+    }
     auto cta_pos = [&](int bb, long long& p0, long long& p1) {
         const int a = static_cast<int>(static_cast<long long>(bb) * nchunks / G);
         const int z = static_cast<int>(static_cast<long long>(bb + 1) * nchunks / G);
@@ -624,13 +655,15 @@ bool MgHierarchy::build(const HostModel& m, const std::vector<int>& colp, const 
         p1 = 32LL * std::min(MG_CHUNK_SLICES * z, nslices);
     };
 
-    // ---- level-0 free rows and pattern (real off-diagonal slots to free columns)
-    std::vector<char> fixed(static_cast<size_t>(m.N), 0);
-    for (int v : m.bc_list) fixed[static_cast<size_t>(v - 1)] = 1;
+    // ---- level-0 free rows (the solver's own node flags: bit0 fluid-connected,
+    // bit2 fixed pressure) and pattern (real off-diagonal slots to free columns)
+    std::vector<uint8_t> nflag(static_cast<size_t>(m.N), 0);
+    MG_CUDA_OK(cudaMemcpy(nflag.data(), d_nflag, nflag.size(), cudaMemcpyDeviceToHost));
     std::vector<uint8_t> free0(static_cast<size_t>(NP), 0);
     for (int p = 0; p < NP; ++p) {
         const int node = P.row_node[static_cast<size_t>(p)];
-        free0[static_cast<size_t>(p)] = node >= 0 && m.tf[static_cast<size_t>(node)] && !fixed[static_cast<size_t>(node)];
+        free0[static_cast<size_t>(p)] = node >= 0 && (nflag[static_cast<size_t>(node)] & 1) &&
+                                        !(nflag[static_cast<size_t>(node)] & 4);
     }
     LevelPattern cur;
     cur.n = NP;
@@ -694,20 +727,23 @@ bool MgHierarchy::build(const HostModel& m, const std::vector<int>& colp, const 
         int w = 0;
         for (int I = 0; I < nn; ++I) w = std::max(w, static_cast<int>(ocol[static_cast<size_t>(I)].size()));
         W[static_cast<size_t>(l) + 1] = w;
-        // outputs: nn*w off-diagonal slots then nn diagonals
-        std::vector<long long> gp(static_cast<size_t>(nn) * w + nn + 1, 0);
-        std::vector<int> ge;
-        std::vector<int> colv(static_cast<size_t>(nn) * w, -1);
-        long long o = 0;
+        // outputs: mg_slots(nn, w) off-diagonal slots (in slot order) then nn diagonals
+        const long long ns = mg_slots(nn, w);
+        std::vector<const std::vector<int>*> at(static_cast<size_t>(ns), nullptr);
+        std::vector<int> colv(static_cast<size_t>(ns), -1);
         for (int I = 0; I < nn; ++I)
-            for (int k = 0; k < w; ++k, ++o) {
-                if (k < static_cast<int>(ocol[static_cast<size_t>(I)].size())) {
-                    colv[static_cast<size_t>(o)] = ocol[static_cast<size_t>(I)][static_cast<size_t>(k)];
-                    const auto& src = osrc[static_cast<size_t>(I)][static_cast<size_t>(k)];
-                    ge.insert(ge.end(), src.begin(), src.end());
-                }
-                gp[static_cast<size_t>(o) + 1] = static_cast<long long>(ge.size());
+            for (int k = 0; k < static_cast<int>(ocol[static_cast<size_t>(I)].size()); ++k) {
+                const long long s = mg_slot(I, k, w);
+                colv[static_cast<size_t>(s)] = ocol[static_cast<size_t>(I)][static_cast<size_t>(k)];
+                at[static_cast<size_t>(s)] = &osrc[static_cast<size_t>(I)][static_cast<size_t>(k)];
             }
+        std::vector<long long> gp(static_cast<size_t>(ns) + nn + 1, 0);
+        std::vector<int> ge;
+        long long o = 0;
+        for (; o < ns; ++o) {
+            if (at[static_cast<size_t>(o)]) ge.insert(ge.end(), at[static_cast<size_t>(o)]->begin(), at[static_cast<size_t>(o)]->end());
+            gp[static_cast<size_t>(o) + 1] = static_cast<long long>(ge.size());
+        }
         for (int I = 0; I < nn; ++I, ++o) {
             ge.insert(ge.end(), dsrc[static_cast<size_t>(I)].begin(), dsrc[static_cast<size_t>(I)].end());
             gp[static_cast<size_t>(o) + 1] = static_cast<long long>(ge.size());
@@ -724,7 +760,7 @@ bool MgHierarchy::build(const HostModel& m, const std::vector<int>& colp, const 
         for (int I = 0; I < nn; ++I) {
             for (int k = 0; k < static_cast<int>(ocol[static_cast<size_t>(I)].size()); ++k) {
                 nx.col.push_back(ocol[static_cast<size_t>(I)][static_cast<size_t>(k)]);
-                nx.sid.push_back(I * w + k);
+                nx.sid.push_back(static_cast<int>(mg_slot(I, k, w)));
             }
             nx.rptr[static_cast<size_t>(I) + 1] = static_cast<int>(nx.col.size());
         }
@@ -747,7 +783,7 @@ bool MgHierarchy::build(const HostModel& m, const std::vector<int>& colp, const 
             cols.assign(colp.begin() + a0, colp.begin() + a1);
             std::sort(cols.begin(), cols.end());
             cols.erase(std::unique(cols.begin(), cols.end()), cols.end());
-            if (cols.size() > 65535) return false;
+            if (cols.size() > 65535) { why = "a CTA halo exceeds 65,535 rows"; return false; }
             for (long long t = a0; t < a1; ++t)
                 lcol[static_cast<size_t>(t)] = static_cast<unsigned short>(
                     std::lower_bound(cols.begin(), cols.end(), colp[static_cast<size_t>(t)]) - cols.begin());
@@ -774,7 +810,7 @@ bool MgHierarchy::build(const HostModel& m, const std::vector<int>& colp, const 
         auto& lc = clcol[static_cast<size_t>(l)];
         hp.assign(static_cast<size_t>(G) + 1, 0);
         ho.assign(static_cast<size_t>(G), 0);
-        lc.assign(static_cast<size_t>(pl.n) * w, 0xffff);
+        lc.assign(static_cast<size_t>(mg_slots(pl.n, w)), 0xffff);
         std::vector<int> cols;
         for (int bb = 0; bb < G; ++bb) {
             long long p0, p1;
@@ -789,15 +825,15 @@ bool MgHierarchy::build(const HostModel& m, const std::vector<int>& colp, const 
             }
             std::sort(cols.begin(), cols.end());
             cols.erase(std::unique(cols.begin(), cols.end()), cols.end());
-            if (cols.size() > 65535) return false;
+            if (cols.size() > 65535) { why = "a CTA halo exceeds 65,535 rows"; return false; }
             ho[static_cast<size_t>(bb)] =
                 o < e ? static_cast<int>(std::lower_bound(cols.begin(), cols.end(), o) - cols.begin()) : 0;
             for (int I = o; I < e; ++I)
                 for (int k = 0; k < w; ++k) {
-                    const int J = lvcol[static_cast<size_t>(l)][static_cast<size_t>(I) * w + k];
+                    const size_t s = static_cast<size_t>(mg_slot(I, k, w));
+                    const int J = lvcol[static_cast<size_t>(l)][s];
                     if (J >= 0)
-                        lc[static_cast<size_t>(I) * w + k] = static_cast<unsigned short>(
-                            std::lower_bound(cols.begin(), cols.end(), J) - cols.begin());
+                        lc[s] = static_cast<unsigned short>(std::lower_bound(cols.begin(), cols.end(), J) - cols.begin());
                 }
             hi.insert(hi.end(), cols.begin(), cols.end());
             hp[static_cast<size_t>(bb) + 1] = static_cast<int>(hi.size());
@@ -805,11 +841,11 @@ bool MgHierarchy::build(const HostModel& m, const std::vector<int>& colp, const 
         }
     }
 
-    // ---- shared memory: doubles (level 0: 4 per halo entry; coarse: 3 per
+    // ---- shared memory: doubles (level 0: 3 per halo entry; coarse: 3 per
     // halo entry; coarsest r and x), then ints (halo rows), then the level-0
     // slot columns
     const int nc = n[static_cast<size_t>(Lc)];
-    long long sd = 4LL * hmax0;
+    long long sd = 3LL * hmax0;
     for (int l = 1; l < Lc; ++l) {
         h_lv[static_cast<size_t>(l)].sd = static_cast<int>(sd);
         sd += 3LL * chmax[static_cast<size_t>(l)];
@@ -822,12 +858,17 @@ bool MgHierarchy::build(const HostModel& m, const std::vector<int>& colp, const 
         si += chmax[static_cast<size_t>(l)];
     }
     smem = static_cast<size_t>(sd) * 8 + static_cast<size_t>(si) * 4 + static_cast<size_t>(smax) * 2 + 16;
-    if (smem > 212 * 1024) return false;
+    // 227 KB per CTA, less the kernel's static shared memory (< 5 KB)
+    if (smem > 222 * 1024) {
+        why = "shared memory " + std::to_string(smem / 1024) + " KB per CTA exceeds 222 KB";
+        return false;
+    }
     const void* fn = fn_mg(rmax);
     int per = 0;
     if (pcg_raise_smem_limit(fn, smem) != cudaSuccess ||
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, fn, MG_NT, smem) != cudaSuccess || per * sms < G) {
         cudaGetLastError();
+        why = "the solver kernel does not fit one CTA per SM with its shared memory";
         return false;
     }
 
@@ -846,7 +887,7 @@ bool MgHierarchy::build(const HostModel& m, const std::vector<int>& colp, const 
         L.W = w;
         L.tpr = level_tpr(l);
         L.col = upload(lvcol[static_cast<size_t>(l)]);
-        L.val = zeros<double>(static_cast<size_t>(nl) * w + nl);
+        L.val = zeros<double>(static_cast<size_t>(mg_slots(nl, w)) + nl);
         L.wd = zeros<double>(static_cast<size_t>(nl));
         L.rho = zeros<double>(static_cast<size_t>(nl));
         L.x = zeros<double>(static_cast<size_t>(nl));
@@ -895,7 +936,7 @@ void MgHierarchy::setup(const double* d_val, const double* pdiag, const int* row
             const MgLevelDev& Lp = h_lv[static_cast<size_t>(l) - 1];
             k_mg_galerkin<<<static_cast<unsigned>((no + T - 1) / T), T, 0, st>>>(
                 d_gptr[static_cast<size_t>(l)], d_gent[static_cast<size_t>(l)], no, Lp.val,
-                Lp.val + static_cast<size_t>(Lp.n) * Lp.W, nullptr, L.val);
+                Lp.val + mg_slots(Lp.n, Lp.W), nullptr, L.val);
         }
         if (l < Lc) k_mg_weights<<<(L.n + T - 1) / T, T, 0, st>>>(L.val, L.col, L.n, L.W, L.wd);
     }

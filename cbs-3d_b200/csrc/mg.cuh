@@ -34,6 +34,16 @@ namespace cbs3d {
 constexpr int MG_MAX_LEVELS = 8;
 constexpr int MG_COARSE_MAX = 160;
 
+// Slot of entry k of row I in a coarse level's off-diagonal arrays: rows in
+// groups of 32, column-major within a group, so a warp reading entry k of 32
+// consecutive rows makes one coalesced 256-byte (FP64) load.
+__host__ __device__ __forceinline__ long long mg_slot(int I, int k, int W)
+{
+    return ((long long)(I >> 5) * W + k) * 32 + (I & 31);
+}
+// Off-diagonal slots of a level of n rows (the diagonal values follow them).
+__host__ __device__ __forceinline__ long long mg_slots(int n, int W) { return (long long)((n + 31) >> 5) * 32 * W; }
+
 // One coarse level l >= 1 on the device.  Rows of level l are the
 // aggregates of level l-1: row I holds rows 8I..8I+7 of level l-1.
 struct MgLevelDev {
@@ -42,15 +52,15 @@ struct MgLevelDev {
     int tpr;                     // threads per row in the solver kernel (fixed per level)
     int sd, si;                  // offsets of the level's halo arrays in the kernel's shared memory
                                  // (doubles: r, weight, staged values; ints: halo rows)
-    const int* col;              // n*W columns (-1 padding)
-    double* val;                 // n*W off-diagonal values, then n diagonal values
+    const int* col;              // mg_slots(n, W) columns (-1 padding), at mg_slot(I, k, W)
+    double* val;                 // mg_slots(n, W) off-diagonal values, then n diagonal values
     double* wd;                  // n: smoother weight / diagonal (0 on rows without free children)
     double* rho;                 // n: residual after pre-smoothing
     double* x;                   // n: correction after post-smoothing
     const int* hptr;             // G+1: every CTA's halo list (own rows and their columns)
     const int* hidx;
     const int* hown;             // G: index of the CTA's first own row in its halo list
-    const unsigned short* lcol;  // n*W: halo-local index of every column (0xffff padding)
+    const unsigned short* lcol;  // mg_slots(n, W): halo-local index of every column (0xffff padding)
     int hmax;                    // largest halo
 };
 
@@ -71,10 +81,13 @@ struct MgDev {
 // Host side: built once per mesh, set up (values) once per solve.
 class MgHierarchy {
 public:
-    // False (hierarchy unusable, nothing allocated) when the mesh does not
-    // fit the register-tiled kernel or the shared memory.
-    bool build(const HostModel& m, const std::vector<int>& colp, const long long* d_slice_off,
-               const int* d_slice_w, const int* d_colp, int device, int sms, int blocks_override);
+    // False when the mesh does not fit the register-tiled kernel or the
+    // shared memory (the reason in `why`; release() frees what was allocated).
+    // d_nflag: the solver's node flags on the device (bit0 fluid-connected,
+    // bit2 fixed pressure), which decide the free rows.
+    bool build(const HostModel& m, const std::vector<int>& colp, const uint8_t* d_nflag,
+               const long long* d_slice_off, const int* d_slice_w, const int* d_colp, int device, int sms,
+               int blocks_override);
     void release();
     // Coarse values, smoother weights and the coarsest inverse from the
     // assembled level-0 operator (d_val, row-position slots) and the
@@ -88,6 +101,7 @@ public:
 
     int G = 0, rmax = 0, Lc = 0, nchunks = 0;
     size_t smem = 0;
+    std::string why;             // why build() declined the mesh
     std::vector<int> n;          // rows per level
     std::vector<int> W;          // off-diagonal width per level (level 0: SELL, unused)
     long long nnz0 = 0;          // real off-diagonal entries of level 0
@@ -99,8 +113,8 @@ private:
     std::vector<void*> allocs;
     template <typename T> T* upload(const std::vector<T>& v);
     template <typename T> T* zeros(size_t count);
-    // Galerkin index lists per level l+1: for every output (n*W off-diagonal
-    // slots, then n diagonal entries) the ordered source entries of level l
+    // Galerkin index lists per level l+1: for every output (mg_slots(n, W)
+    // off-diagonal slots, then n diagonal entries) the ordered source entries of level l
     // (>= 0: off-diagonal slot of level l; < 0: diagonal of row -(id+1)).
     std::vector<long long*> d_gptr;
     std::vector<int*> d_gent;

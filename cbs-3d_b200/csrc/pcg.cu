@@ -295,43 +295,46 @@ __global__ void __launch_bounds__(PCG_THREADS, PCG_CTAS_PER_SM) k_pcg64(PcgDev D
             const uint8_t f = D.nflag[i];
             const bool freen = (f & 1) && !(f & 4);
             double off = 0.0, pci;
-            // four slots' columns and coefficients are loaded before their
-            // gathers, so each lane keeps more loads in flight (the sum still
-            // runs over the slots in order)
-            if (upd) {
-                for (int k0 = 0; k0 < w; k0 += 4) {
-                    int c[4];
-                    double v[4];
+            // Rounds of eight slots; the next round's columns and
+            // coefficients (streamed from HBM on large meshes) are requested
+            // before this round's neighbour gathers (mostly L2 hits), so the
+            // two latencies overlap and each lane keeps more loads in flight.
+            // The sum still runs over the slots in order.
+            constexpr int CH = 8;
+            int cn[CH];
+            double vn[CH];
 #pragma unroll
-                    for (int u = 0; u < 4; ++u) {
-                        c[u] = k0 + u < w ? D.col[base + 32LL * (k0 + u)] : i;
-                        v[u] = k0 + u < w ? D.val[base + 32LL * (k0 + u)] : 0.0;
-                    }
-                    double x[4];
+            for (int u = 0; u < CH; ++u) {
+                cn[u] = u < w ? D.col[base + 32LL * u] : i;
+                vn[u] = u < w ? __ldcs(D.val + base + 32LL * u) : 0.0;
+            }
+            for (int k0 = 0; k0 < w; k0 += CH) {
+                int c[CH];
+                double v[CH];
 #pragma unroll
-                    for (int u = 0; u < 4; ++u) x[u] = fma(beta, __ldcg(pp + c[u]), __ldcg(D.z + c[u]));
+                for (int u = 0; u < CH; ++u) { c[u] = cn[u]; v[u] = vn[u]; }
 #pragma unroll
-                    for (int u = 0; u < 4; ++u)
-                        if (k0 + u < w) off = fma(v[u], x[u], off);
+                for (int u = 0; u < CH; ++u) {
+                    const int k = k0 + CH + u;
+                    cn[u] = k < w ? D.col[base + 32LL * k] : i;
+                    vn[u] = k < w ? __ldcs(D.val + base + 32LL * k) : 0.0;
                 }
+                double x[CH];
+                if (upd) {
+#pragma unroll
+                    for (int u = 0; u < CH; ++u) x[u] = fma(beta, __ldcg(pp + c[u]), __ldcg(D.z + c[u]));
+                } else {
+#pragma unroll
+                    for (int u = 0; u < CH; ++u) x[u] = __ldcg(pc + c[u]);
+                }
+#pragma unroll
+                for (int u = 0; u < CH; ++u)
+                    if (k0 + u < w) off = fma(v[u], x[u], off);
+            }
+            if (upd) {
                 pci = freen ? fma(beta, pp[i], D.z[i]) : 0.0;
                 pc[i] = pci;
             } else {
-                for (int k0 = 0; k0 < w; k0 += 4) {
-                    int c[4];
-                    double v[4];
-#pragma unroll
-                    for (int u = 0; u < 4; ++u) {
-                        c[u] = k0 + u < w ? D.col[base + 32LL * (k0 + u)] : i;
-                        v[u] = k0 + u < w ? D.val[base + 32LL * (k0 + u)] : 0.0;
-                    }
-                    double x[4];
-#pragma unroll
-                    for (int u = 0; u < 4; ++u) x[u] = __ldcg(pc + c[u]);
-#pragma unroll
-                    for (int u = 0; u < 4; ++u)
-                        if (k0 + u < w) off = fma(v[u], x[u], off);
-                }
                 pci = pc[i];
             }
             const double qi = freen ? fma(D.pdiag[i], pci, off) : 0.0;
@@ -2314,6 +2317,10 @@ void PcgEngine::init(const HostModel& m, const uint8_t* nflag, const double* pfi
         d_val32 = dalloc<float>(static_cast<size_t>(nslots));
         d_f32 = dalloc<float>(8 * n);
         CUDA_OK(cudaMemset(d_f32, 0, 8 * n * sizeof(float)));
+    } else if (multigrid) {
+        // FP32 copies of the coefficients for the multigrid cycle's smoothing products
+        d_val32 = dalloc<float>(static_cast<size_t>(nslots));
+        CUDA_OK(cudaMemset(d_val32, 0, static_cast<size_t>(nslots ? nslots : 1) * sizeof(float)));
     }
     d_nflag = nflag;
     d_pfix = pfix;
@@ -2448,7 +2455,7 @@ void PcgEngine::init(const HostModel& m, const uint8_t* nflag, const double* pfi
         mgh = new MgHierarchy;
         bool ok = false;
         try {
-            ok = mgh->build(m, colp, d_slice_off, d_slice_w, d_col, device, sms, blocks_override);
+            ok = mgh->build(m, colp, nflag, d_slice_off, d_slice_w, d_col, device, sms, blocks_override);
         } catch (...) {
             mgh->release();
             delete mgh;
@@ -2456,6 +2463,9 @@ void PcgEngine::init(const HostModel& m, const uint8_t* nflag, const double* pfi
             throw;
         }
         if (!ok) {
+            // the caller asked for multigrid: say why it runs Jacobi-PCG instead
+            std::fprintf(stderr, "cbs3d: multigrid preconditioner unavailable for this mesh (%s); "
+                                 "Jacobi-PCG is used\n", mgh->why.c_str());
             mgh->release();
             delete mgh;
             mgh = nullptr;

@@ -9,11 +9,21 @@
 namespace cbs3d {
 namespace {
 
-// dst = src, 16 bytes per thread per step, grid-stride
+// dst = src: four independent 16-byte loads per thread per step (all issued
+// before the stores), grid-stride, so the copy is bandwidth- rather than
+// latency-bound
 __global__ void __launch_bounds__(512) k_copy_probe(const double2* __restrict__ src, double2* __restrict__ dst, long long n)
 {
     const long long stride = (long long)gridDim.x * blockDim.x;
-    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) dst[i] = __ldcg(src + i);
+    long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    for (; i + 3 * stride < n; i += 4 * stride) {
+        double2 a[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) a[u] = __ldcg(src + i + u * stride);
+#pragma unroll
+        for (int u = 0; u < 4; ++u) dst[i + u * stride] = a[u];
+    }
+    for (; i < n; i += stride) dst[i] = __ldcg(src + i);
 }
 
 }  // namespace
