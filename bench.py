@@ -29,8 +29,9 @@ element-by-element form's 64*E_f + 73*N (FP64) is reported beside them for
 context only, since the assembled operator moves fewer bytes.  achieved =
 bytes per iteration x iterations / the PCG launches' CUDA-event time.  At
 64^3 the operator and vectors (~50 MB) stay in the 126 MB L2, so "roofline"
-is stated against the L2 copy bandwidth measured in this run (a copy of a
-2 x 24 MiB buffer pair, cbs3d_probe_copy_bandwidth), with the grid
+is stated against the L2 read bandwidth measured in this run (200 passes
+over a 48 MiB buffer in one launch, cbs3d_probe_bandwidth; the PCG's L2
+traffic is almost all reads), with the grid
 all-reduce latency (cbs3d_probe_allreduce) as the per-iteration floor;
 "hbm_case" runs the same FP64 engine on a 96^3 cavity, whose per-iteration
 traffic exceeds L2, against the measured HBM copy bandwidth.
@@ -156,29 +157,32 @@ def probes(device: int) -> dict:
 
     from cbs3d import gpu
     L = gpu.lib()
-    L.cbs3d_probe_copy_bandwidth.argtypes = [ctypes.c_int, ctypes.c_longlong, ctypes.c_int,
-                                             ctypes.POINTER(ctypes.c_double)]
+    L.cbs3d_probe_bandwidth.argtypes = [ctypes.c_int, ctypes.c_longlong, ctypes.c_int, ctypes.c_int,
+                                        ctypes.POINTER(ctypes.c_double)]
     L.cbs3d_probe_allreduce.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_double)]
-    l2, hbm, ar = ctypes.c_double(), ctypes.c_double(), ctypes.c_double()
     out = {}
-    if L.cbs3d_probe_copy_bandwidth(device, 24 << 20, 100, ctypes.byref(l2)) == 0:
-        out["l2_copy_gbs"] = l2.value
-    if L.cbs3d_probe_copy_bandwidth(device, 1 << 30, 10, ctypes.byref(hbm)) == 0:
-        out["hbm_copy_gbs"] = hbm.value
+    for key, nbytes, passes, mode in (("l2_read_gbs", 48 << 20, 200, 0), ("l2_copy_gbs", 24 << 20, 200, 1),
+                                      ("hbm_read_gbs", 1 << 30, 10, 0), ("hbm_copy_gbs", 1 << 30, 5, 1)):
+        v = ctypes.c_double()
+        if L.cbs3d_probe_bandwidth(device, nbytes, passes, mode, ctypes.byref(v)) == 0:
+            out[key] = v.value
+    ar = ctypes.c_double()
     if L.cbs3d_probe_allreduce(device, 4000, ctypes.byref(ar)) == 0:
         out["allreduce_us"] = ar.value
     return out
 
 
-def ncu_traffic(kernel: str, n: int):
-    """DRAM bytes (read + write) of one PCG launch from the committed ncu
-    summary, if one exists for this kernel and mesh size."""
+def ncu_traffic(kernel: str, n: int, its_per_launch: float):
+    """DRAM bytes (read + write) of one PCG launch: the committed ncu figure
+    per iteration for this kernel and mesh size (profiles/pcg_traffic.json)
+    times this run's iterations per launch; None without a capture."""
     path = os.path.join(ROOT, "profiles", "pcg_traffic.json")
     if not os.path.exists(path):
         return None
     with open(path) as f:
         d = json.load(f)
-    return d.get(kernel, {}).get(str(n))
+    per_it = d.get(kernel, {}).get(str(n))
+    return None if per_it is None else per_it * its_per_launch
 
 
 # ----------------------------------------------------------- CPU baseline
@@ -303,14 +307,16 @@ def roofline(st, warm, nelem_fluid, npoin, mixed, n, pr, bound="l2"):
     achieved = its * kb / st.pcg_seconds / 1e9 if st.pcg_seconds > 0 and its > 0 else None
     kname = KERNELS.get(st.pcg_kernel, "?")
     if bound == "l2":
-        peak = pr.get("l2_copy_gbs")
-        src = ("measured in this run: copy of a 2 x 24 MiB L2-resident buffer pair "
-               "(cbs3d_probe_copy_bandwidth, CUDA events)")
+        peak = pr.get("l2_read_gbs")
+        src = ("measured in this run: 200 read passes over a 48 MiB L2-resident buffer in one launch "
+               "(cbs3d_probe_bandwidth, CUDA events)")
     else:
         peak, src = hbm, hbm_kind
     out = {"bound": bound, "achieved": achieved, "peak": peak, "unit": "GB/s",
-           "frac": achieved / peak if achieved and peak else None, "traffic": ncu_traffic(kname, n),
-           "traffic_unit": "DRAM bytes per launch (one pressure solve), ncu",
+           "frac": achieved / peak if achieved and peak else None,
+           "traffic": ncu_traffic(kname, n, its / max(st.pcg_launches, 1)),
+           "traffic_unit": "DRAM bytes per launch (one pressure solve): ncu bytes per iteration x this run's "
+                           "iterations per launch",
            "kernel": f"{kname} (persistent PCG, one launch per pressure solve)", "peak_source": src,
            "kernel_bytes_per_iteration": kb, "ebe_bytes_per_iteration": ebe_bytes(nelem_fluid, npoin, mixed),
            "iterations": its, "us_per_iteration": 1e6 * st.pcg_seconds / its if its > 0 else None,

@@ -272,22 +272,17 @@ __global__ void __launch_bounds__(MG_NT, 1) k_pcg_mg(PcgDev D, MgDev M)
         r[k] = p[k] = z[k] = dg[k] = wd[k] = 0.0;
         fr[k] = false;
     }
-    // off[k] = sum_j A_ij src[j] over the own rows' off-diagonal slots, from
-    // the FP64 coefficients or (the cycle's smoothing products, when the
-    // engine keeps them) their FP32 copies
-    auto offdiag = [&](const double* src, double* off, bool fp32 = false) {
+    // off[k] = sum_j A_ij src[j] over the own rows' off-diagonal slots
+    auto offdiag = [&](const double* src, double* off) {
 #pragma unroll
         for (int k = 0; k < RMAX; ++k) off[k] = 0.0;
-        const bool f32 = fp32 && D.val32 != nullptr;
         for (int k0 = 0; k0 < wmax; k0 += 2) {
             double v[RMAX][2];
 #pragma unroll
             for (int k = 0; k < RMAX; ++k)
 #pragma unroll
-                for (int u = 0; u < 2; ++u) {
-                    const long long t = S0 + lbase[k] + 32 * (k0 + u);
-                    v[k][u] = (k0 + u < wr[k]) ? (f32 ? (double)__ldcg(D.val32 + t) : __ldcg(D.val + t)) : 0.0;
-                }
+                for (int u = 0; u < 2; ++u)
+                    v[k][u] = (k0 + u < wr[k]) ? __ldcg(D.val + S0 + lbase[k] + 32 * (k0 + u)) : 0.0;
 #pragma unroll
             for (int k = 0; k < RMAX; ++k)
 #pragma unroll
@@ -306,7 +301,7 @@ __global__ void __launch_bounds__(MG_NT, 1) k_pcg_mg(PcgDev D, MgDev M)
         // (the halo's smoother weights are read through L1: constant per solve)
         for (int k = threadIdx.x; k < nh; k += MG_NT) vh[k] = __ldg(M.wd0 + hidx[k]) * rh[k];
         __syncthreads();
-        offdiag(vh, off, true);
+        offdiag(vh, off);
 #pragma unroll
         for (int k = 0; k < RMAX; ++k) {
             const int i = row[k];
@@ -368,10 +363,16 @@ __global__ void __launch_bounds__(MG_NT, 1) k_pcg_mg(PcgDev D, MgDev M)
                 rc[I] = s;
             }
             __syncthreads();
-            for (int I = threadIdx.x; I < M.nc; I += MG_NT) {
+            // four threads per row (columns sub, sub+4, ... in order, then a
+            // fixed xor tree); every warp runs the same number of rounds
+            for (int I0 = 0; I0 < M.nc; I0 += MG_NT / 4) {
+                const int I = I0 + (threadIdx.x >> 2), sub = threadIdx.x & 3;
                 double x = 0.0;
-                for (int J = 0; J < M.nc; ++J) x = fma(__ldg(M.ainv + (size_t)I * M.nc + J), rc[J], x);
-                xc[I] = x;
+                if (I < M.nc)
+                    for (int J = sub; J < M.nc; J += 4) x = fma(__ldg(M.ainv + (size_t)I * M.nc + J), rc[J], x);
+                x += __shfl_xor_sync(0xffffffffu, x, 1);
+                x += __shfl_xor_sync(0xffffffffu, x, 2);
+                if (I < M.nc && sub == 0) xc[I] = x;
             }
             __syncthreads();
         }
@@ -421,7 +422,7 @@ __global__ void __launch_bounds__(MG_NT, 1) k_pcg_mg(PcgDev D, MgDev M)
             vh[k] = w > 0.0 ? fma(w, rh[k], MG_OVER * xcg) : 0.0;
         }
         __syncthreads();
-        offdiag(vh, off, true);
+        offdiag(vh, off);
 #pragma unroll
         for (int k = 0; k < RMAX; ++k) {
             const int i = row[k];

@@ -2317,10 +2317,6 @@ void PcgEngine::init(const HostModel& m, const uint8_t* nflag, const double* pfi
         d_val32 = dalloc<float>(static_cast<size_t>(nslots));
         d_f32 = dalloc<float>(8 * n);
         CUDA_OK(cudaMemset(d_f32, 0, 8 * n * sizeof(float)));
-    } else if (multigrid) {
-        // FP32 copies of the coefficients for the multigrid cycle's smoothing products
-        d_val32 = dalloc<float>(static_cast<size_t>(nslots));
-        CUDA_OK(cudaMemset(d_val32, 0, static_cast<size_t>(nslots ? nslots : 1) * sizeof(float)));
     }
     d_nflag = nflag;
     d_pfix = pfix;

@@ -397,16 +397,18 @@ cbs3d_status cbs3d_selftest_wait_timeout(int device, int* observed_status);
 cbs3d_status cbs3d_coarse_inverse(int device, int g, const double* a, double* ainv, int variant);
 
 /* Measurement probes (no reference counterpart) that the benchmark uses to
- * state the solver kernels' rooflines.  cbs3d_probe_copy_bandwidth: GB/s of
- * a copy between two device buffers of `bytes` each (read + write bytes over
- * the CUDA-event time of `reps` launches after three warm-up launches): a
- * pair that fits in L2 gives the L2 copy bandwidth, a larger one the HBM copy
- * bandwidth.  cbs3d_probe_allreduce: microseconds per grid-wide all-reduce
+ * state the solver kernels' rooflines.  cbs3d_probe_bandwidth: GB/s of
+ * `passes` passes over a device buffer of `bytes` inside one launch (after a
+ * one-pass warm-up launch), mode 0 reading it, mode 1 copying it to a second
+ * buffer (read + write bytes counted); a buffer that fits in L2 gives the L2
+ * bandwidth, a larger one the HBM bandwidth.  Back-to-back launches cost
+ * about 4 us each on B200, so the passes run inside one launch.
+ * cbs3d_probe_allreduce: microseconds per grid-wide all-reduce
  * of the persistent PCG kernel's kind (one 512-thread CTA per SM, five
  * values, `iters` dependent all-reduces in one cooperative launch) -- the
  * per-iteration latency floor of the single-reduction PCG.  Both allocate
  * and free their own device memory. */
-cbs3d_status cbs3d_probe_copy_bandwidth(int device, long long bytes, int reps, double* gbs);
+cbs3d_status cbs3d_probe_bandwidth(int device, long long bytes, int passes, int mode, double* gbs);
 cbs3d_status cbs3d_probe_allreduce(int device, int iters, double* us_per_allreduce);
 
 #ifdef __cplusplus

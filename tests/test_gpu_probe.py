@@ -1,6 +1,7 @@
-"""The measurement probes the benchmark states its rooflines with: the copy
-bandwidth of an L2-resident buffer pair exceeds that of an HBM-sized pair,
-and a grid all-reduce of the persistent PCG kernel takes microseconds."""
+"""The measurement probes the benchmark states its rooflines with: reading a
+buffer that fits in L2 is faster than reading one that does not, HBM reads
+and copies land in the B200's range, and a grid all-reduce of the persistent
+PCG kernel takes microseconds."""
 import ctypes
 
 import pytest
@@ -8,17 +9,32 @@ import pytest
 pytestmark = pytest.mark.gpu
 
 
-def test_copy_bandwidth_l2_above_hbm():
+def _bw(nbytes, passes, mode):
     from cbs3d import gpu
     L = gpu.lib()
-    L.cbs3d_probe_copy_bandwidth.argtypes = [ctypes.c_int, ctypes.c_longlong, ctypes.c_int,
-                                             ctypes.POINTER(ctypes.c_double)]
-    l2, hbm = ctypes.c_double(), ctypes.c_double()
-    assert L.cbs3d_probe_copy_bandwidth(0, 24 << 20, 50, ctypes.byref(l2)) == 0
-    assert L.cbs3d_probe_copy_bandwidth(0, 1 << 30, 5, ctypes.byref(hbm)) == 0
-    print(f"copy GB/s: L2-resident {l2.value:.0f}, HBM {hbm.value:.0f}")
-    assert 2000.0 < hbm.value < 9000.0
-    assert l2.value > 1.2 * hbm.value
+    L.cbs3d_probe_bandwidth.argtypes = [ctypes.c_int, ctypes.c_longlong, ctypes.c_int, ctypes.c_int,
+                                        ctypes.POINTER(ctypes.c_double)]
+    v = ctypes.c_double()
+    assert L.cbs3d_probe_bandwidth(0, nbytes, passes, mode, ctypes.byref(v)) == 0
+    return v.value
+
+
+def test_bandwidth_l2_above_hbm():
+    l2r, hbmr = _bw(48 << 20, 200, 0), _bw(1 << 30, 10, 0)
+    l2c, hbmc = _bw(24 << 20, 200, 1), _bw(1 << 30, 5, 1)
+    print(f"read GB/s: L2 {l2r:.0f} HBM {hbmr:.0f}; copy GB/s: L2 {l2c:.0f} HBM {hbmc:.0f}")
+    assert 3000.0 < hbmr < 9000.0 and 3000.0 < hbmc < 9000.0
+    assert l2r > 1.2 * hbmr
+
+
+def test_bad_probe_arguments_rejected():
+    from cbs3d import gpu
+    L = gpu.lib()
+    L.cbs3d_probe_bandwidth.argtypes = [ctypes.c_int, ctypes.c_longlong, ctypes.c_int, ctypes.c_int,
+                                        ctypes.POINTER(ctypes.c_double)]
+    v = ctypes.c_double()
+    assert L.cbs3d_probe_bandwidth(0, 1 << 20, 1, 7, ctypes.byref(v)) == 1
+    assert L.cbs3d_probe_bandwidth(0, 100, 1, 0, ctypes.byref(v)) == 1
 
 
 def test_allreduce_latency():
