@@ -228,6 +228,13 @@ __device__ __forceinline__ void cg_finish(const PcgDev& D, const SegView& g, int
 }
 
 // ---------------------------------------------------- persistent FP64 PCG
+// HALO: the neighbour values of each iteration's product (z and the previous
+// direction of every column of the CTA's rows) are staged in shared memory
+// once per iteration, and the slots carry 16-bit indices into that halo
+// (D.halo_ptr/halo_idx/lcol of this kernel's partition), so the rounds
+// stream only coefficients and local columns and read neighbours from shared
+// memory.  Same arithmetic in the same order as without.
+template <bool HALO>
 __global__ void __launch_bounds__(PCG_THREADS, PCG_CTAS_PER_SM) k_pcg64(PcgDev D)
 {
     const SegView g = seg_view<false>(D);
@@ -236,7 +243,11 @@ __global__ void __launch_bounds__(PCG_THREADS, PCG_CTAS_PER_SM) k_pcg64(PcgDev D
     const int s_beg = g.s0 + (int)((long long)b * (g.s1 - g.s0) / G);
     const int s_end = g.s0 + (int)((long long)(b + 1) * (g.s1 - g.s0) / G);
     int phase = 0;
-    
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    double* hz = reinterpret_cast<double*>(smem_raw);   // HALO: z of the halo
+    double* hp = hz + D.halo_max;                       // HALO: previous (first iteration: current) direction
+    const int h0 = HALO ? D.halo_ptr[b] : 0;
+    const int nh = HALO ? D.halo_ptr[b + 1] - h0 : 0;
 
     // ---- r0 = b - A p0, z0, d0 = z0, (r,r), (r,z), max|r|
     Acc4 acc{0.0, 0.0, 0.0, 0.0};
@@ -288,6 +299,16 @@ __global__ void __launch_bounds__(PCG_THREADS, PCG_CTAS_PER_SM) k_pcg64(PcgDev D
         // ---- q = A p (p formed here from z and the previous p), (p, q)
         Acc4 pa{0.0, 0.0, 0.0, 0.0};
         const bool upd = it > 1;
+        if constexpr (HALO) {
+            // z and pp (or pc) were written before the last all-reduce
+            __syncthreads();
+            for (int k = threadIdx.x; k < nh; k += PCG_THREADS) {
+                const int j = D.halo_idx[h0 + k];
+                hz[k] = upd ? __ldcg(D.z + j) : 0.0;
+                hp[k] = __ldcg((upd ? pp : pc) + j);
+            }
+            __syncthreads();
+        }
         for (int s = s_beg + warp; s < s_end; s += PCG_WARPS) {
             const int i = s * 32 + lane;
             const long long base = D.slice_off[s] + lane;
@@ -301,11 +322,14 @@ __global__ void __launch_bounds__(PCG_THREADS, PCG_CTAS_PER_SM) k_pcg64(PcgDev D
             // two latencies overlap and each lane keeps more loads in flight.
             // The sum still runs over the slots in order.
             constexpr int CH = 8;
+            // columns: global positions, or (HALO) indices into the staged halo
+            auto colat = [&](long long t) -> int { return HALO ? (int)__ldcs(D.lcol + t) : D.col[t]; };
+            const int cpad = HALO ? 0 : i;   // a valid column for the padding lanes of a round
             int cn[CH];
             double vn[CH];
 #pragma unroll
             for (int u = 0; u < CH; ++u) {
-                cn[u] = u < w ? D.col[base + 32LL * u] : i;
+                cn[u] = u < w ? colat(base + 32LL * u) : cpad;
                 vn[u] = u < w ? __ldcs(D.val + base + 32LL * u) : 0.0;
             }
             for (int k0 = 0; k0 < w; k0 += CH) {
@@ -316,11 +340,19 @@ __global__ void __launch_bounds__(PCG_THREADS, PCG_CTAS_PER_SM) k_pcg64(PcgDev D
 #pragma unroll
                 for (int u = 0; u < CH; ++u) {
                     const int k = k0 + CH + u;
-                    cn[u] = k < w ? D.col[base + 32LL * k] : i;
+                    cn[u] = k < w ? colat(base + 32LL * k) : cpad;
                     vn[u] = k < w ? __ldcs(D.val + base + 32LL * k) : 0.0;
                 }
                 double x[CH];
-                if (upd) {
+                if constexpr (HALO) {
+                    if (upd) {
+#pragma unroll
+                        for (int u = 0; u < CH; ++u) x[u] = fma(beta, hp[c[u]], hz[c[u]]);
+                    } else {
+#pragma unroll
+                        for (int u = 0; u < CH; ++u) x[u] = hp[c[u]];
+                    }
+                } else if (upd) {
 #pragma unroll
                     for (int u = 0; u < CH; ++u) x[u] = fma(beta, __ldcg(pp + c[u]), __ldcg(D.z + c[u]));
                 } else {
@@ -2337,7 +2369,7 @@ void PcgEngine::init(const HostModel& m, const uint8_t* nflag, const double* pfi
     };
     rmax = 0;
     variant = 1;
-    nblocks = grid_for(reinterpret_cast<const void*>(k_pcg64));
+    nblocks = grid_for(reinterpret_cast<const void*>(k_pcg64<false>));
     const int rm[4] = {1, 2, 4, 8};
     if (kernel_choice == 0 || kernel_choice == 3 || kernel_choice == 4) {
         const void* hc3[4] = {reinterpret_cast<const void*>(k_pcg64h<1>), reinterpret_cast<const void*>(k_pcg64h<2>),
@@ -2445,6 +2477,47 @@ void PcgEngine::init(const HostModel& m, const uint8_t* nflag, const double* pfi
             const int per_cta = (nslices + g - 1) / g;
             if ((per_cta + PCG_WARPS - 1) / PCG_WARPS <= rm[c]) { rmax = rm[c]; nblocks = g; variant = 2; break; }
         }
+    }
+    if (variant == 1 && N > 0) {
+        // the global-vector kernel with its neighbour values staged in shared
+        // memory, when every CTA's halo fits (up to about 100^3 hexes)
+        const int g = nblocks;
+        std::vector<int> hptr(static_cast<size_t>(g) + 1, 0), hidx, cols;
+        std::vector<unsigned short> lcol(static_cast<size_t>(nslots), 0);
+        int hmax = 0;
+        bool fits = true;
+        for (int bb = 0; bb < g && fits; ++bb) {
+            const int sb = static_cast<int>(static_cast<long long>(bb) * nslices / g);
+            const int se = static_cast<int>(static_cast<long long>(bb + 1) * nslices / g);
+            const long long a0 = P.slice_off[static_cast<size_t>(sb)], a1 = P.slice_off[static_cast<size_t>(se)];
+            cols.assign(colp.begin() + a0, colp.begin() + a1);
+            std::sort(cols.begin(), cols.end());
+            cols.erase(std::unique(cols.begin(), cols.end()), cols.end());
+            if (cols.size() > 65535 || cols.size() * 16 + 16 > 220 * 1024) { fits = false; break; }
+            for (long long t = a0; t < a1; ++t)
+                lcol[static_cast<size_t>(t)] = static_cast<unsigned short>(
+                    std::lower_bound(cols.begin(), cols.end(), colp[static_cast<size_t>(t)]) - cols.begin());
+            hidx.insert(hidx.end(), cols.begin(), cols.end());
+            hptr[static_cast<size_t>(bb) + 1] = static_cast<int>(hidx.size());
+            hmax = std::max(hmax, static_cast<int>(cols.size()));
+        }
+        const void* fh = reinterpret_cast<const void*>(k_pcg64<true>);
+        const size_t smem = static_cast<size_t>(hmax) * 16 + 16;
+        int per = 0;
+        if (fits && raise_smem_limit(fh, smem) == cudaSuccess &&
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, fh, PCG_THREADS, smem) == cudaSuccess && per * sms >= g) {
+            d_halo_ptr = dalloc<int>(hptr.size());
+            d_halo_idx = dalloc<int>(hidx.size());
+            d_lcol = dalloc<unsigned short>(lcol.size());
+            CUDA_OK(cudaMemcpy(d_halo_ptr, hptr.data(), hptr.size() * sizeof(int), cudaMemcpyHostToDevice));
+            CUDA_OK(cudaMemcpy(d_halo_idx, hidx.data(), hidx.size() * sizeof(int), cudaMemcpyHostToDevice));
+            CUDA_OK(cudaMemcpy(d_lcol, lcol.data(), lcol.size() * sizeof(unsigned short), cudaMemcpyHostToDevice));
+            dev_halo_max = hmax;
+            global_halo = true;
+            global_halo_smem = smem;
+            global_halo_total = static_cast<long long>(hidx.size());
+        }
+        cudaGetLastError();
     }
     if (two_level && variant == 4 && nthreads == 512 && !mixed_ok) build_coarse(m, colp);
     if (multigrid && !mixed && !coarse) {
@@ -2570,8 +2643,8 @@ cbs3d_status PcgEngine::solve(double* pres, double* rhs1, double* pdiag, int pre
     CUDA_OK(cudaMemsetAsync(d_bar, 0, 4 * sizeof(unsigned), st));
     CUDA_OK(cudaMemsetAsync(d_out, 0, sizeof(CgOut), st));
     void* args[] = {&D};
-    const void* fn = reinterpret_cast<const void*>(k_pcg64);
-    size_t smem = 0;
+    const void* fn = global_halo ? reinterpret_cast<const void*>(k_pcg64<true>) : reinterpret_cast<const void*>(k_pcg64<false>);
+    size_t smem = global_halo ? global_halo_smem : 0;
     if (variant == 2) {
         if (rmax == 1) fn = reinterpret_cast<const void*>(k_pcg64r<1>);
         else if (rmax == 2) fn = reinterpret_cast<const void*>(k_pcg64r<2>);
@@ -2674,7 +2747,12 @@ size_t PcgEngine::bytes_per_iter() const
     }
     // Phase A: coefficient + column per pair entry; z and previous p of the
     // row (16 B), pdiag (8), new p written (8), q written (8), node flag (1).
-    // Phase B: q, r, pres, pdiag read (32), r, pres, z written (24).
+    // Phase B: q, r, pres, pdiag read (32), r, pres, z written (24).  With the
+    // shared-memory halo the columns are 16-bit and every halo entry's z and
+    // previous p are read once per iteration.
+    if (global_halo)
+        return static_cast<size_t>(nnz_offdiag) * 10 + static_cast<size_t>(N) * 97 +
+               static_cast<size_t>(global_halo_total) * 16;
     return static_cast<size_t>(nnz_offdiag) * 12 + static_cast<size_t>(N) * 97;
 }
 

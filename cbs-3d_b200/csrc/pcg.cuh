@@ -133,6 +133,9 @@ public:
     void build_coarse(const HostModel& m, const std::vector<int>& colp);
     void coarse_setup(const double* pdiag, const int* row_node, cudaStream_t st);
     int variant = 1;         // 1 global vectors, 2 register rows, 3 + shared-memory halo, 4 + one sync per iteration
+    bool global_halo = false;     // variant 1 with its neighbour values staged in shared memory
+    size_t global_halo_smem = 0;
+    long long global_halo_total = 0;   // halo entries over all CTAs
     size_t halo_smem = 0;    // dynamic shared memory of the halo kernel
     size_t cgcg_smem = 0;    // ... of the CG-CG kernel (halo + its rows' pressure and diagonal)
     int cgcg_xs_off = 0;     // where those rows start (0: kept in global memory)
