@@ -244,8 +244,9 @@ __global__ void __launch_bounds__(PCG_THREADS, PCG_CTAS_PER_SM) k_pcg64(PcgDev D
     const int s_end = g.s0 + (int)((long long)(b + 1) * (g.s1 - g.s0) / G);
     int phase = 0;
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    double* hz = reinterpret_cast<double*>(smem_raw);   // HALO: z of the halo
-    double* hp = hz + D.halo_max;                       // HALO: previous (first iteration: current) direction
+    // HALO: per halo entry (z, previous direction) -- on the first
+    // iteration (0, current direction) -- one 16-byte read per neighbour
+    double2* hzp = reinterpret_cast<double2*>(smem_raw);
     const int h0 = HALO ? D.halo_ptr[b] : 0;
     const int nh = HALO ? D.halo_ptr[b + 1] - h0 : 0;
 
@@ -304,8 +305,7 @@ __global__ void __launch_bounds__(PCG_THREADS, PCG_CTAS_PER_SM) k_pcg64(PcgDev D
             __syncthreads();
             for (int k = threadIdx.x; k < nh; k += PCG_THREADS) {
                 const int j = D.halo_idx[h0 + k];
-                hz[k] = upd ? __ldcg(D.z + j) : 0.0;
-                hp[k] = __ldcg((upd ? pp : pc) + j);
+                hzp[k] = make_double2(upd ? __ldcg(D.z + j) : 0.0, __ldcg((upd ? pp : pc) + j));
             }
             __syncthreads();
         }
@@ -347,10 +347,13 @@ __global__ void __launch_bounds__(PCG_THREADS, PCG_CTAS_PER_SM) k_pcg64(PcgDev D
                 if constexpr (HALO) {
                     if (upd) {
 #pragma unroll
-                        for (int u = 0; u < CH; ++u) x[u] = fma(beta, hp[c[u]], hz[c[u]]);
+                        for (int u = 0; u < CH; ++u) {
+                            const double2 zp = hzp[c[u]];
+                            x[u] = fma(beta, zp.y, zp.x);
+                        }
                     } else {
 #pragma unroll
-                        for (int u = 0; u < CH; ++u) x[u] = hp[c[u]];
+                        for (int u = 0; u < CH; ++u) x[u] = hzp[c[u]].y;
                     }
                 } else if (upd) {
 #pragma unroll

@@ -34,6 +34,9 @@ def test_bench_line_contract():
     assert roof["kernel_bytes_per_iteration"] > 0 and roof["allreduce_us"] > 0
     hbm = d["hbm_case"]
     assert hbm["bound"] == "hbm" and hbm["achieved"] > 0 and abs(hbm["frac"] - hbm["achieved"] / hbm["peak"]) < 1e-9
+    # a fraction above ~1 would mean the byte model overstates what the kernel moves
+    for r in (roof, hbm, d["multigrid"]["roofline"]):
+        assert 0.0 < r["frac"] <= 1.2, r
     e2e = d["e2e"]
     assert e2e["value"] > 0 and e2e["h2d_bytes_per_step"] > 0 and e2e["d2h_bytes_per_step"] > 0
     assert d["gpu_launches"] > 0
