@@ -247,8 +247,9 @@ __global__ void __launch_bounds__(PCG_THREADS, PCG_CTAS_PER_SM) k_pcg64(PcgDev D
     // HALO: per halo entry (z, previous direction) -- on the first
     // iteration (0, current direction) -- one 16-byte read per neighbour
     double2* hzp = reinterpret_cast<double2*>(smem_raw);
-    const int h0 = HALO ? D.halo_ptr[b] : 0;
-    const int nh = HALO ? D.halo_ptr[b + 1] - h0 : 0;
+    // HALO: the CTA's slices in KP parts (one unless a CTA's whole halo
+    // would not fit), each staged and processed in turn
+    const int KP = HALO ? (D.halo_parts > 0 ? D.halo_parts : 1) : 1;
 
     // ---- r0 = b - A p0, z0, d0 = z0, (r,r), (r,z), max|r|
     Acc4 acc{0.0, 0.0, 0.0, 0.0};
@@ -300,16 +301,20 @@ __global__ void __launch_bounds__(PCG_THREADS, PCG_CTAS_PER_SM) k_pcg64(PcgDev D
         // ---- q = A p (p formed here from z and the previous p), (p, q)
         Acc4 pa{0.0, 0.0, 0.0, 0.0};
         const bool upd = it > 1;
+        for (int part = 0; part < KP; ++part) {
+        const int ps0 = s_beg + (int)((long long)part * (s_end - s_beg) / KP);
+        const int ps1 = s_beg + (int)((long long)(part + 1) * (s_end - s_beg) / KP);
         if constexpr (HALO) {
             // z and pp (or pc) were written before the last all-reduce
             __syncthreads();
+            const int h0 = D.halo_ptr[b * KP + part], nh = D.halo_ptr[b * KP + part + 1] - h0;
             for (int k = threadIdx.x; k < nh; k += PCG_THREADS) {
                 const int j = D.halo_idx[h0 + k];
                 hzp[k] = make_double2(upd ? __ldcg(D.z + j) : 0.0, __ldcg((upd ? pp : pc) + j));
             }
             __syncthreads();
         }
-        for (int s = s_beg + warp; s < s_end; s += PCG_WARPS) {
+        for (int s = ps0 + warp; s < ps1; s += PCG_WARPS) {
             const int i = s * 32 + lane;
             const long long base = D.slice_off[s] + lane;
             const int w = D.slice_w[s];
@@ -376,6 +381,7 @@ __global__ void __launch_bounds__(PCG_THREADS, PCG_CTAS_PER_SM) k_pcg64(PcgDev D
             D.q[i] = qi;
             if (freen) pa.a = fma(pci, qi, pa.a);
         }
+        }   // parts
         t = Acc4{0.0, 0.0, 0.0, 0.0};
         if (!grid_allreduce(pa, D, g, phase, t)) return;
         ++phase;
@@ -2483,26 +2489,38 @@ void PcgEngine::init(const HostModel& m, const uint8_t* nflag, const double* pfi
     }
     if (variant == 1 && N > 0) {
         // the global-vector kernel with its neighbour values staged in shared
-        // memory, when every CTA's halo fits (up to about 100^3 hexes)
+        // memory: each CTA's slices in the fewest parts (at most 8) whose
+        // halos fit
         const int g = nblocks;
-        std::vector<int> hptr(static_cast<size_t>(g) + 1, 0), hidx, cols;
+        std::vector<int> hptr, hidx, cols;
         std::vector<unsigned short> lcol(static_cast<size_t>(nslots), 0);
         int hmax = 0;
-        bool fits = true;
-        for (int bb = 0; bb < g && fits; ++bb) {
-            const int sb = static_cast<int>(static_cast<long long>(bb) * nslices / g);
-            const int se = static_cast<int>(static_cast<long long>(bb + 1) * nslices / g);
-            const long long a0 = P.slice_off[static_cast<size_t>(sb)], a1 = P.slice_off[static_cast<size_t>(se)];
-            cols.assign(colp.begin() + a0, colp.begin() + a1);
-            std::sort(cols.begin(), cols.end());
-            cols.erase(std::unique(cols.begin(), cols.end()), cols.end());
-            if (cols.size() > 65535 || cols.size() * 16 + 16 > 220 * 1024) { fits = false; break; }
-            for (long long t = a0; t < a1; ++t)
-                lcol[static_cast<size_t>(t)] = static_cast<unsigned short>(
-                    std::lower_bound(cols.begin(), cols.end(), colp[static_cast<size_t>(t)]) - cols.begin());
-            hidx.insert(hidx.end(), cols.begin(), cols.end());
-            hptr[static_cast<size_t>(bb) + 1] = static_cast<int>(hidx.size());
-            hmax = std::max(hmax, static_cast<int>(cols.size()));
+        bool fits = false;
+        for (int kp = 1; kp <= 8 && !fits; ++kp) {
+            hptr.assign(static_cast<size_t>(g) * kp + 1, 0);
+            hidx.clear();
+            hmax = 0;
+            fits = true;
+            for (int bb = 0; bb < g && fits; ++bb) {
+                const int sb = static_cast<int>(static_cast<long long>(bb) * nslices / g);
+                const int se = static_cast<int>(static_cast<long long>(bb + 1) * nslices / g);
+                for (int q = 0; q < kp && fits; ++q) {
+                    const int pb = sb + static_cast<int>(static_cast<long long>(q) * (se - sb) / kp);
+                    const int pe = sb + static_cast<int>(static_cast<long long>(q + 1) * (se - sb) / kp);
+                    const long long a0 = P.slice_off[static_cast<size_t>(pb)], a1 = P.slice_off[static_cast<size_t>(pe)];
+                    cols.assign(colp.begin() + a0, colp.begin() + a1);
+                    std::sort(cols.begin(), cols.end());
+                    cols.erase(std::unique(cols.begin(), cols.end()), cols.end());
+                    if (cols.size() > 65535 || cols.size() * 16 + 16 > 220 * 1024) { fits = false; break; }
+                    for (long long t = a0; t < a1; ++t)
+                        lcol[static_cast<size_t>(t)] = static_cast<unsigned short>(
+                            std::lower_bound(cols.begin(), cols.end(), colp[static_cast<size_t>(t)]) - cols.begin());
+                    hidx.insert(hidx.end(), cols.begin(), cols.end());
+                    hptr[static_cast<size_t>(bb) * kp + q + 1] = static_cast<int>(hidx.size());
+                    hmax = std::max(hmax, static_cast<int>(cols.size()));
+                }
+            }
+            if (fits) global_halo_parts = kp;
         }
         const void* fh = reinterpret_cast<const void*>(k_pcg64<true>);
         const size_t smem = static_cast<size_t>(hmax) * 16 + 16;
@@ -2562,6 +2580,7 @@ void PcgEngine::init(const HostModel& m, const uint8_t* nflag, const double* pfi
     dev.part = d_part; dev.bar = d_bar; dev.status = d_status; dev.out = d_out;
     dev.halo_ptr = d_halo_ptr; dev.halo_idx = d_halo_idx; dev.lcol = d_lcol; dev.halo_max = dev_halo_max;
     dev.xs_off = cgcg_xs_off;
+    dev.halo_parts = global_halo ? global_halo_parts : 0;
     dev.row_node = d_row_node;
 }
 

@@ -66,6 +66,8 @@ struct PcgDev {
     const PcgInst* inst;         // batched launch: instance descriptors (else null)
     int xs_off;                  // CG-CG kernel: byte offset in shared memory of its rows' pressure
                                  // and diagonal (2*RMAX*threads doubles); 0: read from global memory
+    int halo_parts;              // global-vector kernel with a shared-memory halo: parts per CTA, each
+                                 // with its own halo (halo_ptr indexed by CTA*parts + part)
 };
 
 class MgHierarchy;
@@ -136,6 +138,7 @@ public:
     bool global_halo = false;     // variant 1 with its neighbour values staged in shared memory
     size_t global_halo_smem = 0;
     long long global_halo_total = 0;   // halo entries over all CTAs
+    int global_halo_parts = 1;         // parts per CTA, each with its own halo
     size_t halo_smem = 0;    // dynamic shared memory of the halo kernel
     size_t cgcg_smem = 0;    // ... of the CG-CG kernel (halo + its rows' pressure and diagonal)
     int cgcg_xs_off = 0;     // where those rows start (0: kept in global memory)

@@ -80,3 +80,21 @@ def test_config_full_size_vs_reference(name, mode):
             _check_fields(case, z, u, p, t, s, tol)
     u, p, t = ctx.fields()
     _check_fields(case, z, u, p, t, "", tol)
+
+
+def test_cavity64_mixed_vs_fp64_200_steps():
+    """The benchmark configuration's mixed-precision form (FP32 PCG
+    iterations, FP64 residual replacement and stopping test) against the
+    FP64 engine over the stated 200 steps of the 64^3 jittered cavity:
+    u and p within 1e-8 relative L2."""
+    from cbs3d import gpu
+    case, _ = _load("cfg2_cavity64")
+    a = gpu.Context(case)
+    a.step(200)
+    b = gpu.Context(case, precision=gpu.MIXED)
+    st = b.step(200)
+    assert st.pcg_kernel == 5
+    (ua, pa, _), (ub, pb, _) = a.fields(), b.fields()
+    eu, ep = rel_l2(ub, ua), rel_l2(pb, pa)
+    print(f"mixed vs FP64 after 200 steps: u {eu:.2e} p {ep:.2e}")
+    assert eu <= EXT_TOL and ep <= EXT_TOL

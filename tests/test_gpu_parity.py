@@ -283,3 +283,23 @@ def test_coarse_inverse_kernels(g):
         a1[g // 2, g // 2] = 1.0
     ref = np.linalg.inv(a1)
     assert np.linalg.norm(r - ref) / np.linalg.norm(ref) <= 1e-12
+
+
+def test_global_kernel_halo_in_parts():
+    """The global-vector PCG with its neighbour values staged in shared
+    memory, in several parts per CTA when a CTA's whole halo does not fit
+    (forced here: the global kernel on 8 CTAs for a 48^3 cavity, ~14,700 rows
+    per CTA): same solutions as the default engine to RUN_TOL, iteration
+    counts within 2."""
+    from cbs3d import cases
+    gpu = _gpu()
+    case = cases.cavity(48, re=400.0, ntime=10 ** 6, jitter=0.15, seed=1234)
+    a = gpu.Context(case)
+    b = gpu.Context(case, pcg_kernel=1, pcg_blocks=8)
+    for _ in range(3):
+        sa, sb = a.step(1), b.step(1)
+        assert sb.pcg_kernel == 1
+        assert abs(sa.cg.iterations - sb.cg.iterations) <= 2
+    (ua, pa, _), (ub, pb, _) = a.fields(), b.fields()
+    assert rel_l2(ub, ua) <= RUN_TOL
+    assert rel_l2(pb, pa) <= RUN_TOL
