@@ -132,18 +132,18 @@ __device__ __forceinline__ double coarse_row(const MgLevelDev& Lv, int I, int su
     double acc = 0.0;
     if (active) {
         const int W = Lv.W;
-        for (int k0 = sub; k0 < W; k0 += 4 * T) {
-            unsigned short lc[4];
-            double v[4];
+        for (int k0 = sub; k0 < W; k0 += 8 * T) {
+            unsigned short lc[8];
+            double v[8];
 #pragma unroll
-            for (int u = 0; u < 4; ++u) {
+            for (int u = 0; u < 8; ++u) {
                 const int k = k0 + u * T;
                 const long long s = mg_slot(I, k < W ? k : 0, W);
                 lc[u] = k < W ? __ldg(Lv.lcol + s) : (unsigned short)0xffffu;
                 v[u] = k < W ? __ldg(Lv.val + s) : 0.0;
             }
 #pragma unroll
-            for (int u = 0; u < 4; ++u)
+            for (int u = 0; u < 8; ++u)
                 if (lc[u] != 0xffffu) acc = fma(v[u], vl[lc[u]], acc);
         }
     }
@@ -231,11 +231,24 @@ __global__ void __launch_bounds__(MG_NT, 1) k_pcg_mg(PcgDev D, MgDev M)
         }
         if (!sync_grid()) return false;
         double t4[4] = {0.0, 0.0, 0.0, 0.0};
-        for (int c = threadIdx.x; c < M.nchunks; c += MG_NT)
-            for (int q = 0; q < NV; ++q) {
-                const double y = __ldcg(part + (size_t)q * M.nchunks + c);
-                t4[q] = q < NS ? t4[q] + y : fmax(t4[q], y);
-            }
+        // four chunks per round, all their loads issued before the sums
+        // (each thread's chunks are still summed in ascending order)
+        for (int c0 = threadIdx.x; c0 < M.nchunks; c0 += 4 * MG_NT) {
+            double y[4][4];
+#pragma unroll
+            for (int u = 0; u < 4; ++u)
+#pragma unroll
+                for (int q = 0; q < 4; ++q) {
+                    const int c = c0 + u * MG_NT;
+                    y[u][q] = (q < NV && c < M.nchunks) ? __ldcg(part + (size_t)q * M.nchunks + c) : 0.0;
+                }
+#pragma unroll
+            for (int u = 0; u < 4; ++u)
+                if (c0 + u * MG_NT < M.nchunks)
+#pragma unroll
+                    for (int q = 0; q < 4; ++q)
+                        if (q < NV) t4[q] = q < NS ? t4[q] + y[u][q] : fmax(t4[q], y[u][q]);
+        }
         for (int q = 0; q < NV; ++q) {
 #pragma unroll
             for (int o = 16; o > 0; o >>= 1) {
