@@ -42,6 +42,12 @@ constexpr int PCG_WARPS = PCG_THREADS / 32;
 
 #define CUDA_OK(x) do { cudaError_t e_ = (x); if (e_ != cudaSuccess) throw Error(CBS3D_CUDA_ERROR, std::string(#x) + ": " + cudaGetErrorString(e_)); } while (0)
 
+// shared memory of one SM that the CG-CG kernel's CTAs may fill with
+// coefficients (bytes; the B200's 228 KB)
+#ifndef CBS3D_PCG_COEF_CAP
+#define CBS3D_PCG_COEF_CAP (228LL * 1024)
+#endif
+
 // The dynamic shared-memory limit is one attribute per kernel and device,
 // shared by every engine and batch in the process: it only ever grows, so a
 // smaller later request cannot invalidate an earlier engine's launches.
@@ -1031,6 +1037,11 @@ __global__ void __launch_bounds__(NT, NT >= 512 ? 1 : 2) k_pcg64c(PcgDev D)
     double* pds = xs ? xs + RMAX * NT : nullptr;
     for (int k = threadIdx.x; k < nh; k += NT) hidx[k] = D.halo_idx[h0 + k];
     for (int k = threadIdx.x; k < nsl; k += NT) lcs[k] = D.lcol[S0 + k];
+    // the coefficients of the CTA's leading slots, read from shared memory in
+    // every iteration instead of from L2 (whole slices: csm is a multiple of 32)
+    const int csm = D.coef_slots < nsl ? D.coef_slots : nsl;
+    double* cvs = reinterpret_cast<double*>(smem_raw + D.coef_off);
+    for (int k = threadIdx.x; k < csm; k += NT) cvs[k] = __ldcg(D.val + S0 + k);
     int phase = 0;
     const int N = D.N;
     // parity buffers: r in r/pA, w in q/pB, s in z/dz(+N)... laid out by the engine
@@ -1069,8 +1080,10 @@ __global__ void __launch_bounds__(NT, NT >= 512 ? 1 : 2) k_pcg64c(PcgDev D)
 #pragma unroll
             for (int k = 0; k < RMAX; ++k)
 #pragma unroll
-                for (int u = 0; u < CH; ++u)
-                    v[k][u] = (k0 + u < wr[k]) ? __ldcg(D.val + S0 + lbase[k] + 32 * (k0 + u)) : 0.0;
+                for (int u = 0; u < CH; ++u) {
+                    const int t = lbase[k] + 32 * (k0 + u);
+                    v[k][u] = (k0 + u >= wr[k]) ? 0.0 : (t < csm) ? cvs[t] : __ldcg(D.val + S0 + t);
+                }
 #pragma unroll
             for (int k = 0; k < RMAX; ++k)
 #pragma unroll
@@ -2452,6 +2465,31 @@ void PcgEngine::init(const HostModel& m, const uint8_t* nflag, const double* pfi
                 }
                 cudaGetLastError();
             }
+            // the coefficients of each CTA's leading slots in shared memory
+            // beside the halo: as many whole slices as the CTAs of one SM
+            // leave room for
+            cgcg_coef_slots = 0;
+            cgcg_coef_off = 0;
+            if (want == 4) {
+                const long long per_need = (g + sms - 1) / sms;
+                const long long cap = std::min<long long>(227 * 1024, CBS3D_PCG_COEF_CAP / per_need - 1024);
+                const size_t off = (cgcg_smem + 15) & ~static_cast<size_t>(15);
+                long long slots = std::min<long long>((cap - static_cast<long long>(off)) / 8, smax) & ~31LL;
+                while (slots >= 32) {
+                    const size_t with = off + static_cast<size_t>(slots) * 8;
+                    int per2 = 0;
+                    if (raise_smem_limit(fn, with) == cudaSuccess &&
+                        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per2, fn, nt, with) == cudaSuccess &&
+                        per2 * sms >= g) {
+                        cgcg_smem = with;
+                        cgcg_coef_off = static_cast<int>(off);
+                        cgcg_coef_slots = static_cast<int>(slots);
+                        break;
+                    }
+                    slots = (slots / 2) & ~31LL;
+                }
+                cudaGetLastError();
+            }
             d_halo_ptr = dalloc<int>(hptr.size());
             d_halo_idx = dalloc<int>(hidx.size());
             d_lcol = dalloc<unsigned short>(lcol.size());
@@ -2580,6 +2618,8 @@ void PcgEngine::init(const HostModel& m, const uint8_t* nflag, const double* pfi
     dev.part = d_part; dev.bar = d_bar; dev.status = d_status; dev.out = d_out;
     dev.halo_ptr = d_halo_ptr; dev.halo_idx = d_halo_idx; dev.lcol = d_lcol; dev.halo_max = dev_halo_max;
     dev.xs_off = cgcg_xs_off;
+    dev.coef_slots = cgcg_coef_slots;
+    dev.coef_off = cgcg_coef_off;
     dev.halo_parts = global_halo ? global_halo_parts : 0;
     dev.row_node = d_row_node;
 }

@@ -68,6 +68,9 @@ struct PcgDev {
                                  // and diagonal (2*RMAX*threads doubles); 0: read from global memory
     int halo_parts;              // global-vector kernel with a shared-memory halo: parts per CTA, each
                                  // with its own halo (halo_ptr indexed by CTA*parts + part)
+    int coef_slots;              // CG-CG kernel: leading slots of each CTA's range whose coefficients
+                                 // are copied into shared memory for the solve (a multiple of 32)
+    int coef_off;                // byte offset of that copy in shared memory
 };
 
 class MgHierarchy;
@@ -142,6 +145,8 @@ public:
     size_t halo_smem = 0;    // dynamic shared memory of the halo kernel
     size_t cgcg_smem = 0;    // ... of the CG-CG kernel (halo + its rows' pressure and diagonal)
     int cgcg_xs_off = 0;     // where those rows start (0: kept in global memory)
+    int cgcg_coef_slots = 0; // leading slots per CTA whose coefficients sit in shared memory
+    int cgcg_coef_off = 0;   // where they start
     size_t mixed_smem = 0;   // dynamic shared memory of the mixed-precision kernel
     bool mixed_ok = false;   // mixed precision runs on the FP32 kernel (else FP64)
     int dev_slot_max = 0;
