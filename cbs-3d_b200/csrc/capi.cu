@@ -21,33 +21,6 @@
 
 using namespace cbs3d;
 
-
-namespace {
-
-// Records one step: dtreal, the PCG result, hb, rtime; tags a pending failure
-// with the step counter.
-__global__ void k_step_log(DevState S, const CgOut* cg, double* log, int* counter, int cap)
-{
-    if (threadIdx.x != 0 || blockIdx.x != 0) return;
-    const int k = *counter;
-    *counter = k + 1;
-    if (S.status->code != 0 && S.status->step == 0) S.status->step = k + 1;
-    if (k >= cap) return;
-    double* r = log + (size_t)k * LOG_FIELDS;
-    r[0] = S.dscal[0];
-    r[1] = cg->iterations;
-    r[2] = cg->initial_l2;
-    r[3] = cg->final_l2;
-    r[4] = cg->rel;
-    r[5] = cg->max_abs;
-    r[6] = cg->converged;
-    for (int q = 0; q < 15; ++q) r[7 + q] = S.dscal[2 + q];
-    r[22] = S.dscal[1];
-    r[23] = cg->outer;
-}
-
-}  // namespace
-
 std::string cbs3d::reason_text(const DevStatus& s)
 {
     const std::string at = std::to_string(s.where);
@@ -179,6 +152,7 @@ void cbs3d_ctx::setup(bool own_pcg)
     S.elbuf = buf.alloc<double>(16 * E);   // Step 1: 4 records of 4 doubles per tet; others use 12*E
     S.dscal = buf.alloc<double>(32);
     S.dtmin_bits = buf.alloc<unsigned long long>(1);
+    S.conv_count = buf.alloc<unsigned>(1);
     S.status = buf.alloc<DevStatus>(1);
     conv_blocks = static_cast<int>(nb(static_cast<long long>(N)));
     S.red = buf.alloc<double>(static_cast<size_t>(conv_blocks) * 16);
@@ -191,6 +165,7 @@ void cbs3d_ctx::setup(bool own_pcg)
     CUDA_OK(cudaMemset(S.dscal, 0, 32 * sizeof(double)));
     CUDA_OK(cudaMemset(S.status, 0, sizeof(DevStatus)));
     CUDA_OK(cudaMemset(d_counter, 0, sizeof(int)));
+    CUDA_OK(cudaMemset(S.conv_count, 0, sizeof(unsigned)));
 
     // Preprocess on the device (Solver::initialise geometry and mass).
     k_geometry<<<nb(m.E), T, 0, st>>>(S);
@@ -286,15 +261,15 @@ void cbs3d_ctx::enqueue_post(int it)
         k_step4_elem<<<nb(m.E), T, 0, st>>>(S);
         k_step4_node<<<nb(m.N), T, 0, st>>>(S);
     }
-    k_conv_partial<<<static_cast<unsigned>(conv_blocks), T, 0, st>>>(S);
-    k_conv_finish<<<1, 15 * 32, 0, st>>>(S, conv_blocks);
-    k_step_log<<<1, 32, 0, st>>>(S, batch_out ? batch_out : pcg.d_out, d_log, d_counter, log_cap);
+    k_conv_partial<<<static_cast<unsigned>(conv_blocks), T, 0, st>>>(S, batch_out ? batch_out : pcg.d_out, d_log,
+                                                                    d_counter, log_cap);
 }
 
 int cbs3d_ctx::kernels_outside_solve(int it) const
 {
-    // begin, timestep, dt_finish, lhs, step1 x2, step2 x2, step3 x2, conv x2, log (13)
-    return 13 + (!fixed_dt(it) && force_global() ? 1 : 0) + (m.p.step2_check > 0 ? 2 : 0) +
+    // begin, timestep, dt_finish, lhs, step1 x2, step2 x2, step3 x2,
+    // convergence (with the step log): 11
+    return 11 + (!fixed_dt(it) && force_global() ? 1 : 0) + (m.p.step2_check > 0 ? 2 : 0) +
            (m.temp_calc > 0 ? 2 : 0);
 }
 
@@ -770,8 +745,7 @@ cbs3d_status cbs3d_run_stage(cbs3d_ctx* c, const char* stage)
         else if (s == "step3") { k_step3_elem<<<nb(m.E), T, 0, st>>>(S); k_step3_node<<<nb(m.N), T, 0, st>>>(S); }
         else if (s == "step4") { if (m.temp_calc > 0) { k_step4_elem<<<nb(m.E), T, 0, st>>>(S); k_step4_node<<<nb(m.N), T, 0, st>>>(S); } }
         else if (s == "convergence") {
-            k_conv_partial<<<static_cast<unsigned>(c->conv_blocks), T, 0, st>>>(S);
-            k_conv_finish<<<1, 15 * 32, 0, st>>>(S, c->conv_blocks);
+            k_conv_partial<<<static_cast<unsigned>(c->conv_blocks), T, 0, st>>>(S, nullptr, nullptr, nullptr, 0);
         } else throw Error(CBS3D_INVALID_INPUT, "unknown stage: " + s);
         CUDA_OK(cudaGetLastError());
         CUDA_OK(cudaStreamSynchronize(st));

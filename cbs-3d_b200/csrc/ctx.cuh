@@ -20,7 +20,6 @@
 namespace cbs3d {
 
 constexpr int T = 256;
-constexpr int LOG_FIELDS = 24;   // dtreal, cg[6], hb[15], rtime, spare
 
 inline unsigned nb(long long n, int t = T) { return static_cast<unsigned>((n + t - 1) / t); }
 

@@ -24,6 +24,18 @@ struct DevStatus {
     int step;      // step counter value when the failure was first seen (0 = not yet)
 };
 
+// Result of one pressure solve, written by the PCG kernels.
+struct CgOut {
+    int iterations;
+    int converged;
+    int outer;
+    int pad;
+    double initial_l2, final_l2, rel, max_abs;
+};
+
+// doubles per step in the step log: dtreal, cg[6], hb[15], rtime, outer
+constexpr int LOG_FIELDS = 24;
+
 enum Stage {
     ST_GEOM = 1, ST_MASS, ST_TIMESTEP, ST_LHS, ST_STEP1, ST_STEP2RHS, ST_PCG, ST_STEP3, ST_STEP4,
     ST_CONV, ST_DTCORR
@@ -83,6 +95,7 @@ struct DevState {
     // scalars
     double* dscal;              // [0] dtreal (as double), [1] rtime, [2..16] hb
     unsigned long long* dtmin_bits;
+    unsigned* conv_count;       // k_conv_partial blocks done (the last one resets it)
     DevStatus* status;
     double* red;                // reduction partials
 };

@@ -23,8 +23,7 @@ __global__ void k_step3_elem(DevState S);
 __global__ void k_step3_node(DevState S);
 __global__ void k_step4_elem(DevState S);
 __global__ void k_step4_node(DevState S);
-__global__ void k_conv_partial(DevState S);
-__global__ void k_conv_finish(DevState S, int nblocks);
+__global__ void k_conv_partial(DevState S, const CgOut* cg, double* log, int* counter, int cap);
 __global__ void k_gstif(DevState S, double* out);
 __global__ void k_matvec_color(DevState S, const int* color_elem, int beg, int end, const double* gst,
                                const double* x, double* y);

@@ -887,9 +887,12 @@ __global__ void k_step4_node(DevState S)
 // ====================================================== convergence norms
 // Solver::updateVelocityMagnitude (src/solver/Solver.cpp:689-699) and the
 // per-node sums of Convergence::evaluate (src/solver/Convergence.cpp:276-317),
-// reduced per block in a fixed order; k_conv_finish sums the block partials
-// in block order and finalises (:319-348).
-__global__ void k_conv_partial(DevState S)
+// reduced per block in a fixed order; the last block to finish sums the block
+// partials (for each measure: lanes stride the blocks, then a fixed shuffle
+// tree) and finalises them (:319-348).  With log != nullptr it then records
+// the step: dtreal, the PCG result, hb, rtime, and tags a pending failure
+// with the step counter.
+__global__ void k_conv_partial(DevState S, const CgOut* cg, double* log, int* counter, int cap)
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     double v[15];
@@ -941,42 +944,69 @@ __global__ void k_conv_partial(DevState S)
         double s = 0.0;
         for (int w = 0; w < (int)(blockDim.x >> 5); ++w) s += sm[threadIdx.x][w];
         S.red[(size_t)blockIdx.x * 16 + threadIdx.x] = s;
+        __threadfence();
     }
-}
-
-__global__ void k_conv_finish(DevState S, int nblocks)
-{
-    // one warp per measure, lanes stride the block partials, fixed tree
-    const int q = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    __shared__ int s_last;
     __shared__ double hb[16];
-    if (q < 15) {
+    __syncthreads();
+    if (threadIdx.x == 0) s_last = atomicAdd(S.conv_count, 1u) == gridDim.x - 1;
+    __syncthreads();
+    if (!s_last) return;
+    __threadfence();
+    const int nblocks = (int)gridDim.x, lane = threadIdx.x & 31;
+    for (int q = threadIdx.x >> 5; q < 15; q += (int)(blockDim.x >> 5)) {
         double s = 0.0;
-        for (int b = lane; b < nblocks; b += 32) s += S.red[(size_t)b * 16 + q];
+        int b = lane;
+        for (; b + 7 * 32 < nblocks; b += 8 * 32) {
+            double y[8];
+#pragma unroll
+            for (int u = 0; u < 8; ++u) y[u] = __ldcg(S.red + (size_t)(b + 32 * u) * 16 + q);
+#pragma unroll
+            for (int u = 0; u < 8; ++u) s += y[u];
+        }
+        for (; b < nblocks; b += 32) s += __ldcg(S.red + (size_t)b * 16 + q);
         for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
         if (lane == 0) hb[q] = s;
     }
     __syncthreads();
-    if (threadIdx.x == 0) {
-        double h[15];
-        for (int k = 0; k < 15; ++k) h[k] = hb[k];
-        for (int b = 0; b < 9; b += 3) {
-            h[b] = sqrt(h[b] / (h[b + 1] + 1.0e-30));
-            h[b + 1] = sqrt(h[b + 1]);
-            h[b + 2] = sqrt(h[b + 2]);
-        }
-        h[9] = sqrt(h[9] / (h[10] + 1.0e-30));
-        h[10] = sqrt(h[10]);
-        h[11] = sqrt(h[11]);
-        if (S.P.temp_calc > 0) {
-            h[12] = sqrt(h[12] / (h[13] + 1.0e-30));
-            h[13] = sqrt(h[13]);
-            h[14] = sqrt(h[14]);
-        } else {
-            h[12] = h[13] = h[14] = 0.0;
-        }
-        for (int k = 0; k < 15; ++k) S.dscal[2 + k] = h[k];
+    if (threadIdx.x != 0) return;
+    *S.conv_count = 0;   // for the next launch
+    double h[15];
+    for (int k = 0; k < 15; ++k) h[k] = hb[k];
+    for (int b = 0; b < 9; b += 3) {
+        h[b] = sqrt(h[b] / (h[b + 1] + 1.0e-30));
+        h[b + 1] = sqrt(h[b + 1]);
+        h[b + 2] = sqrt(h[b + 2]);
     }
+    h[9] = sqrt(h[9] / (h[10] + 1.0e-30));
+    h[10] = sqrt(h[10]);
+    h[11] = sqrt(h[11]);
+    if (S.P.temp_calc > 0) {
+        h[12] = sqrt(h[12] / (h[13] + 1.0e-30));
+        h[13] = sqrt(h[13]);
+        h[14] = sqrt(h[14]);
+    } else {
+        h[12] = h[13] = h[14] = 0.0;
+    }
+    for (int k = 0; k < 15; ++k) S.dscal[2 + k] = h[k];
+    if (!log) return;
+    const int k = *counter;
+    *counter = k + 1;
+    if (S.status->code != 0 && S.status->step == 0) S.status->step = k + 1;
+    if (k >= cap) return;
+    double* r = log + (size_t)k * LOG_FIELDS;
+    r[0] = S.dscal[0];
+    r[1] = cg->iterations;
+    r[2] = cg->initial_l2;
+    r[3] = cg->final_l2;
+    r[4] = cg->rel;
+    r[5] = cg->max_abs;
+    r[6] = cg->converged;
+    for (int q = 0; q < 15; ++q) r[7 + q] = h[q];
+    r[22] = S.dscal[1];
+    r[23] = cg->outer;
 }
+
 
 // gstif = gstifE * dt (TimeStep.cpp:873-892), materialised only on request
 __global__ void k_gstif(DevState S, double* out)

@@ -42,12 +42,6 @@ constexpr int PCG_WARPS = PCG_THREADS / 32;
 
 #define CUDA_OK(x) do { cudaError_t e_ = (x); if (e_ != cudaSuccess) throw Error(CBS3D_CUDA_ERROR, std::string(#x) + ": " + cudaGetErrorString(e_)); } while (0)
 
-// shared memory of one SM that the CG-CG kernel's CTAs may fill with
-// coefficients (bytes; the B200's 228 KB)
-#ifndef CBS3D_PCG_COEF_CAP
-#define CBS3D_PCG_COEF_CAP (228LL * 1024)
-#endif
-
 // The dynamic shared-memory limit is one attribute per kernel and device,
 // shared by every engine and batch in the process: it only ever grows, so a
 // smaller later request cannot invalidate an earlier engine's launches.
@@ -1012,7 +1006,7 @@ __device__ __forceinline__ bool grid_allreduce3g(Acc6 v, double x, const PcgDev&
     return ok;
 }
 
-template <int RMAX, bool BATCH, int NT>
+template <int RMAX, bool BATCH, int NT, int KS = 0>
 __global__ void __launch_bounds__(NT, NT >= 512 ? 1 : 2) k_pcg64c(PcgDev D)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -1037,11 +1031,15 @@ __global__ void __launch_bounds__(NT, NT >= 512 ? 1 : 2) k_pcg64c(PcgDev D)
     double* pds = xs ? xs + RMAX * NT : nullptr;
     for (int k = threadIdx.x; k < nh; k += NT) hidx[k] = D.halo_idx[h0 + k];
     for (int k = threadIdx.x; k < nsl; k += NT) lcs[k] = D.lcol[S0 + k];
-    // the coefficients of the CTA's leading slots, read from shared memory in
-    // every iteration instead of from L2 (whole slices: csm is a multiple of 32)
-    const int csm = D.coef_slots < nsl ? D.coef_slots : nsl;
+    // KS = 1: the coefficients of every warp's first row (the CTA's first
+    // NT/32 slices, its leading slots) copied once into shared memory and
+    // read from there in every iteration instead of from L2
     double* cvs = reinterpret_cast<double*>(smem_raw + D.coef_off);
-    for (int k = threadIdx.x; k < csm; k += NT) cvs[k] = __ldcg(D.val + S0 + k);
+    if constexpr (KS > 0) {
+        const int sc = s_beg + (NT / 32) * KS < s_end ? s_beg + (NT / 32) * KS : s_end;
+        const int c0 = (int)(D.slice_off[sc] - S0);
+        for (int k = threadIdx.x; k < c0; k += NT) cvs[k] = __ldcg(D.val + S0 + k);
+    }
     int phase = 0;
     const int N = D.N;
     // parity buffers: r in r/pA, w in q/pB, s in z/dz(+N)... laid out by the engine
@@ -1080,10 +1078,10 @@ __global__ void __launch_bounds__(NT, NT >= 512 ? 1 : 2) k_pcg64c(PcgDev D)
 #pragma unroll
             for (int k = 0; k < RMAX; ++k)
 #pragma unroll
-                for (int u = 0; u < CH; ++u) {
-                    const int t = lbase[k] + 32 * (k0 + u);
-                    v[k][u] = (k0 + u >= wr[k]) ? 0.0 : (t < csm) ? cvs[t] : __ldcg(D.val + S0 + t);
-                }
+                for (int u = 0; u < CH; ++u)
+                    v[k][u] = (k0 + u < wr[k]) ? (k < KS ? cvs[lbase[k] + 32 * (k0 + u)]
+                                                         : __ldcg(D.val + S0 + lbase[k] + 32 * (k0 + u)))
+                                               : 0.0;
 #pragma unroll
             for (int k = 0; k < RMAX; ++k)
 #pragma unroll
@@ -2187,13 +2185,13 @@ namespace {
 
 // Instantiations of the single-reduction kernels by rows per thread, batch
 // mode and CTA size.
-template <bool BATCH, int NT>
+template <bool BATCH, int NT, int KS = 0>
 const void* fn_cgcg(int rmax)
 {
-    return rmax == 1 ? reinterpret_cast<const void*>(k_pcg64c<1, BATCH, NT>)
-         : rmax == 2 ? reinterpret_cast<const void*>(k_pcg64c<2, BATCH, NT>)
-         : rmax == 4 ? reinterpret_cast<const void*>(k_pcg64c<4, BATCH, NT>)
-                     : reinterpret_cast<const void*>(k_pcg64c<8, BATCH, NT>);
+    return rmax == 1 ? reinterpret_cast<const void*>(k_pcg64c<1, BATCH, NT, KS>)
+         : rmax == 2 ? reinterpret_cast<const void*>(k_pcg64c<2, BATCH, NT, KS>)
+         : rmax == 4 ? reinterpret_cast<const void*>(k_pcg64c<4, BATCH, NT, KS>)
+                     : reinterpret_cast<const void*>(k_pcg64c<8, BATCH, NT, KS>);
 }
 template <bool BATCH, int NT>
 const void* fn_mixed(int rmax)
@@ -2210,7 +2208,11 @@ const void* fn_twolevel(int rmax)
          : rmax == 4 ? reinterpret_cast<const void*>(k_pcg64d<4>)
                      : reinterpret_cast<const void*>(k_pcg64d<8>);
 }
-const void* fn_cgcg_single(int rmax, int nt) { return nt == 256 ? fn_cgcg<false, 256>(rmax) : fn_cgcg<false, 512>(rmax); }
+const void* fn_cgcg_single(int rmax, int nt, int ks = 0)
+{
+    if (ks) return nt == 256 ? fn_cgcg<false, 256, 1>(rmax) : fn_cgcg<false, 512, 1>(rmax);
+    return nt == 256 ? fn_cgcg<false, 256>(rmax) : fn_cgcg<false, 512>(rmax);
+}
 const void* fn_mixed_single(int rmax, int nt) { return nt == 256 ? fn_mixed<false, 256>(rmax) : fn_mixed<false, 512>(rmax); }
 
 // The batch runs 256-thread CTAs, two per SM: its instances are small and
@@ -2465,28 +2467,31 @@ void PcgEngine::init(const HostModel& m, const uint8_t* nflag, const double* pfi
                 }
                 cudaGetLastError();
             }
-            // the coefficients of each CTA's leading slots in shared memory
-            // beside the halo: as many whole slices as the CTAs of one SM
-            // leave room for
-            cgcg_coef_slots = 0;
+            // the kernel that reads every warp's first row's coefficients
+            // from shared memory, where the CTAs' first slices fit beside
+            // the halo
+            cgcg_ks = 0;
             cgcg_coef_off = 0;
             if (want == 4) {
+                long long cmax = 0;
+                for (int bb = 0; bb < g; ++bb) {
+                    const int sb = static_cast<int>(static_cast<long long>(bb) * nslices / g);
+                    const int se = static_cast<int>(static_cast<long long>(bb + 1) * nslices / g);
+                    const int sc = std::min(sb + nwarps, se);
+                    cmax = std::max(cmax, P.slice_off[static_cast<size_t>(sc)] - P.slice_off[static_cast<size_t>(sb)]);
+                }
                 const long long per_need = (g + sms - 1) / sms;
-                const long long cap = std::min<long long>(227 * 1024, CBS3D_PCG_COEF_CAP / per_need - 1024);
+                const long long cap = std::min<long long>(227 * 1024, 228 * 1024 / per_need - 1024);
                 const size_t off = (cgcg_smem + 15) & ~static_cast<size_t>(15);
-                long long slots = std::min<long long>((cap - static_cast<long long>(off)) / 8, smax) & ~31LL;
-                while (slots >= 32) {
-                    const size_t with = off + static_cast<size_t>(slots) * 8;
-                    int per2 = 0;
-                    if (raise_smem_limit(fn, with) == cudaSuccess &&
-                        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per2, fn, nt, with) == cudaSuccess &&
-                        per2 * sms >= g) {
-                        cgcg_smem = with;
-                        cgcg_coef_off = static_cast<int>(off);
-                        cgcg_coef_slots = static_cast<int>(slots);
-                        break;
-                    }
-                    slots = (slots / 2) & ~31LL;
+                const size_t with = off + static_cast<size_t>(cmax) * 8;
+                const void* fk = fn_cgcg_single(rm[c], nt, 1);
+                int per2 = 0;
+                if (static_cast<long long>(with) <= cap && raise_smem_limit(fk, with) == cudaSuccess &&
+                    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per2, fk, nt, with) == cudaSuccess &&
+                    per2 * sms >= g) {
+                    cgcg_ks = 1;
+                    cgcg_smem = with;
+                    cgcg_coef_off = static_cast<int>(off);
                 }
                 cudaGetLastError();
             }
@@ -2618,7 +2623,6 @@ void PcgEngine::init(const HostModel& m, const uint8_t* nflag, const double* pfi
     dev.part = d_part; dev.bar = d_bar; dev.status = d_status; dev.out = d_out;
     dev.halo_ptr = d_halo_ptr; dev.halo_idx = d_halo_idx; dev.lcol = d_lcol; dev.halo_max = dev_halo_max;
     dev.xs_off = cgcg_xs_off;
-    dev.coef_slots = cgcg_coef_slots;
     dev.coef_off = cgcg_coef_off;
     dev.halo_parts = global_halo ? global_halo_parts : 0;
     dev.row_node = d_row_node;
@@ -2722,7 +2726,7 @@ cbs3d_status PcgEngine::solve(double* pres, double* rhs1, double* pdiag, int pre
         fn = fn_mixed_single(rmax, nthreads);
         smem = mixed_smem;
     } else if (variant == 4) {
-        fn = fn_cgcg_single(rmax, nthreads);
+        fn = fn_cgcg_single(rmax, nthreads, cgcg_ks);
         smem = cgcg_smem;
     }
     CoarseDev C = cdev;

@@ -12,14 +12,6 @@
 
 namespace cbs3d {
 
-struct CgOut {
-    int iterations;
-    int converged;
-    int outer;
-    int pad;
-    double initial_l2, final_l2, rel, max_abs;
-};
-
 // One instance of a batched solve: CTAs [cta0, cta0+ncta) of the launch own
 // slices [s0, s1); its own scalars, barrier counter, partials, status, result.
 struct PcgInst {
@@ -68,9 +60,8 @@ struct PcgDev {
                                  // and diagonal (2*RMAX*threads doubles); 0: read from global memory
     int halo_parts;              // global-vector kernel with a shared-memory halo: parts per CTA, each
                                  // with its own halo (halo_ptr indexed by CTA*parts + part)
-    int coef_slots;              // CG-CG kernel: leading slots of each CTA's range whose coefficients
-                                 // are copied into shared memory for the solve (a multiple of 32)
-    int coef_off;                // byte offset of that copy in shared memory
+    int coef_off;                // CG-CG kernel with its warps' first rows' coefficients in shared
+                                 // memory: byte offset of that copy
 };
 
 class MgHierarchy;
@@ -145,7 +136,7 @@ public:
     size_t halo_smem = 0;    // dynamic shared memory of the halo kernel
     size_t cgcg_smem = 0;    // ... of the CG-CG kernel (halo + its rows' pressure and diagonal)
     int cgcg_xs_off = 0;     // where those rows start (0: kept in global memory)
-    int cgcg_coef_slots = 0; // leading slots per CTA whose coefficients sit in shared memory
+    int cgcg_ks = 0;         // 1: the kernel reads its warps' first rows' coefficients from shared memory
     int cgcg_coef_off = 0;   // where they start
     size_t mixed_smem = 0;   // dynamic shared memory of the mixed-precision kernel
     bool mixed_ok = false;   // mixed precision runs on the FP32 kernel (else FP64)
