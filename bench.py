@@ -281,7 +281,8 @@ def ebe_bytes(nelem_fluid: int, npoin: int, mixed: bool) -> int:
     return (40 * nelem_fluid + 37 * npoin) if mixed else (64 * nelem_fluid + 73 * npoin)
 
 
-KERNELS = {1: "k_pcg64", 2: "k_pcg64r", 3: "k_pcg64h", 4: "k_pcg64c", 5: "k_pcg32m", 6: "k_pcg64d", 7: "k_pcg_mg"}
+KERNELS = {1: "k_pcg64", 2: "k_pcg64r", 3: "k_pcg64h", 4: "k_pcg64c", 5: "k_pcg32m", 6: "k_pcg64d", 7: "k_pcg_mg",
+           8: "k_pcg64g"}
 
 
 def timed_run(args, ctx, dist):

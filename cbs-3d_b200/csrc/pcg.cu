@@ -1006,6 +1006,251 @@ __device__ __forceinline__ bool grid_allreduce3g(Acc6 v, double x, const PcgDev&
     return ok;
 }
 
+// ------------------------------------ global-vector single-reduction PCG
+// The Chronopoulos-Gear iteration of k_pcg64c for meshes whose rows do not
+// fit the register tiling: the rows' r, s, w (double-buffered by iteration
+// parity), direction p and pressure stay in global memory, and every CTA
+// stages, per part of its slices, the new z of its halo into shared memory
+// from the previous iteration's r, w, s and the inverse diagonal -- the same
+// operations the owner applies to its rows.  One grid all-reduce per
+// iteration (k_pcg64 takes two) and no separate vector-update pass.  The
+// search direction lives in the engine's permuted right-hand side, which is
+// dead once r0 is formed.  Where the whole halo fits (one part) the inverse
+// diagonal of the halo stays in shared memory for the solve.
+__global__ void __launch_bounds__(PCG_THREADS, PCG_CTAS_PER_SM) k_pcg64g(PcgDev D)
+{
+    constexpr int NT = PCG_THREADS;
+    const SegView g = seg_view<false>(D);
+    const int G = g.G, b = g.b;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int s_beg = g.s0 + (int)((long long)b * (g.s1 - g.s0) / G);
+    const int s_end = g.s0 + (int)((long long)(b + 1) * (g.s1 - g.s0) / G);
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int KP = D.halo_parts > 0 ? D.halo_parts : 1;
+    const bool dzres = KP == 1;   // the halo's inverse diagonal resident in shared memory
+    double* vh = reinterpret_cast<double*>(smem_raw);
+    double* dzh = vh + D.halo_max;
+    int phase = 0;
+    const int N = D.N;
+    double* rb[2] = {D.r, D.r + N};
+    double* wb[2] = {D.q, D.q + N};
+    double* sb[2] = {D.pA, D.pB};
+    double* dz = D.z;     // free ? 1/diagonal : 0  (z = r * dz)
+    double* pv = D.rhs1;  // search direction (after r0)
+
+    // halo of part q: h0, nh
+    auto halo_of = [&](int q, int& h0, int& nh) {
+        h0 = D.halo_ptr[b * KP + q];
+        nh = D.halo_ptr[b * KP + q + 1] - h0;
+    };
+    // off-diagonal sum of row s*32+lane over the staged halo: rounds of eight
+    // slots, the next round's local columns and coefficients requested before
+    // this round's shared-memory reads; the sum runs over the slots in order
+    auto offdiag = [&](int s) -> double {
+        const long long base = D.slice_off[s] + lane;
+        const int w = D.slice_w[s];
+        constexpr int CH = 8;
+        double off = 0.0;
+        int cn[CH];
+        double vn[CH];
+#pragma unroll
+        for (int u = 0; u < CH; ++u) {
+            cn[u] = u < w ? (int)__ldcs(D.lcol + base + 32LL * u) : 0;
+            vn[u] = u < w ? __ldcs(D.val + base + 32LL * u) : 0.0;
+        }
+        for (int k0 = 0; k0 < w; k0 += CH) {
+            int c[CH];
+            double v[CH];
+#pragma unroll
+            for (int u = 0; u < CH; ++u) { c[u] = cn[u]; v[u] = vn[u]; }
+#pragma unroll
+            for (int u = 0; u < CH; ++u) {
+                const int k = k0 + CH + u;
+                cn[u] = k < w ? (int)__ldcs(D.lcol + base + 32LL * k) : 0;
+                vn[u] = k < w ? __ldcs(D.val + base + 32LL * k) : 0.0;
+            }
+#pragma unroll
+            for (int u = 0; u < CH; ++u)
+                if (k0 + u < w) off = fma(v[u], vh[c[u]], off);
+        }
+        return off;
+    };
+
+    // ---- phase 0a: r0 = b - A x0 (constraints as the reference), dz, p = s = 0
+    Acc6 acc{0.0, 0.0, 0.0, 0.0, 0.0};
+    for (int part = 0; part < KP; ++part) {
+        const int ps0 = s_beg + (int)((long long)part * (s_end - s_beg) / KP);
+        const int ps1 = s_beg + (int)((long long)(part + 1) * (s_end - s_beg) / KP);
+        int h0, nh;
+        halo_of(part, h0, nh);
+        __syncthreads();
+        for (int k = threadIdx.x; k < nh; k += NT) vh[k] = __ldcg(D.pres + D.halo_idx[h0 + k]);
+        __syncthreads();
+        for (int s = ps0 + warp; s < ps1; s += PCG_WARPS) {
+            const int i = s * 32 + lane;
+            const double off = offdiag(s);
+            const uint8_t f = D.nflag[i];
+            const bool active = f & 1, fr = (f & 1) && !(f & 4);
+            const double pd = D.pdiag[i];
+            const double y = fma(pd, D.pres[i], off);
+            double ri = active ? D.rhs1[i] - y : 0.0;
+            double dd = 0.0;
+            if (!fr) ri = 0.0;
+            if (fr) {
+                if (g.precond) {
+                    if (!(isfinite(pd) && pd > 1.0e-30)) acc.flag = fmax(acc.flag, 1.0);
+                    dd = 1.0 / pd;
+                } else {
+                    dd = 1.0;
+                }
+                if (!isfinite(ri)) acc.flag = fmax(acc.flag, 2.0);
+                acc.c = fma(ri, ri, acc.c);
+                acc.mx = fmax(acc.mx, fabs(ri));
+            }
+            rb[0][i] = ri;
+            dz[i] = dd;
+            sb[0][i] = 0.0;
+        }
+    }
+    Acc6 t{0.0, 0.0, 0.0, 0.0, 0.0};
+    if (!grid_allreduce3<NT>(acc, D, g, phase, t)) return;
+    ++phase;
+    const double init = sqrt(t.c);
+    if (init <= 1.0e-300) { cg_finish(D, g, 0, 1, init, init, 0.0, t.mx); return; }
+    if (cg_converged(g.conv_test, 1.0, t.mx, g.rel_tol, g.abs_tol)) { cg_finish(D, g, 0, 1, init, init, 1.0, t.mx); return; }
+    if (t.flag >= 2.0) { if (b == 0 && threadIdx.x == 0) set_status(seg_status(D, g), 4, ST_PCG, 0, R_PCG_RESID); return; }
+    if (t.flag >= 1.0) { if (b == 0 && threadIdx.x == 0) set_status(seg_status(D, g), 1, ST_PCG, 0, R_PCG_DIAG); return; }
+
+    // ---- phase 0b: z0 = M^-1 r0, w0 = A z0, gamma0 = (r0,z0), delta0 = (z0,w0);
+    // the right-hand side is no longer needed: p = 0 from here
+    acc = Acc6{0.0, 0.0, 0.0, 0.0, 0.0};
+    for (int part = 0; part < KP; ++part) {
+        const int ps0 = s_beg + (int)((long long)part * (s_end - s_beg) / KP);
+        const int ps1 = s_beg + (int)((long long)(part + 1) * (s_end - s_beg) / KP);
+        int h0, nh;
+        halo_of(part, h0, nh);
+        __syncthreads();
+        for (int k = threadIdx.x; k < nh; k += NT) {
+            const int j = D.halo_idx[h0 + k];
+            const double dj = __ldcg(dz + j);
+            if (dzres) dzh[k] = dj;
+            vh[k] = __ldcg(rb[0] + j) * dj;
+        }
+        __syncthreads();
+        for (int s = ps0 + warp; s < ps1; s += PCG_WARPS) {
+            const int i = s * 32 + lane;
+            const double off = offdiag(s);
+            const uint8_t f = D.nflag[i];
+            const bool fr = (f & 1) && !(f & 4);
+            const double ri = rb[0][i];
+            const double zi = ri * dz[i];
+            const double wi = fr ? fma(D.pdiag[i], zi, off) : 0.0;
+            wb[0][i] = wi;
+            pv[i] = 0.0;
+            if (fr) {
+                acc.a = fma(ri, zi, acc.a);
+                acc.b = fma(zi, wi, acc.b);
+            }
+        }
+    }
+    t = Acc6{0.0, 0.0, 0.0, 0.0, 0.0};
+    if (!grid_allreduce3<NT>(acc, D, g, phase, t)) return;
+    ++phase;
+    double gam = t.a;
+    if (gam <= 1.0e-300 || !isfinite(gam)) { if (b == 0 && threadIdx.x == 0) set_status(seg_status(D, g), 3, ST_PCG, 0, R_PCG_RZ0); return; }
+    double den = t.b;
+    double beta = 0.0, fin = init, rel = 1.0, mx = 0.0, alpha = 0.0;
+    int it = 0, conv = 0;
+    for (it = 1; it <= g.max_iter; ++it) {
+        if (fabs(den) <= 1.0e-300 || !isfinite(den)) { if (b == 0 && threadIdx.x == 0) set_status(seg_status(D, g), 3, ST_PCG, it, R_PCG_PAP); return; }
+        alpha = gam / den;
+        const int po = (it - 1) & 1, pn = it & 1;
+        const double* so = sb[po];
+        const double* wo = wb[po];
+        const double* ro = rb[po];
+        Acc6 a6{0.0, 0.0, 0.0, 0.0, 0.0};
+        for (int part = 0; part < KP; ++part) {
+            const int ps0 = s_beg + (int)((long long)part * (s_end - s_beg) / KP);
+            const int ps1 = s_beg + (int)((long long)(part + 1) * (s_end - s_beg) / KP);
+            int h0, nh;
+            halo_of(part, h0, nh);
+            // stage z_it of the halo: s = w_o + beta*s_o, r = r_o - alpha*s,
+            // z = r * dz (SU nodes per thread per round, all loads first); the
+            // all-reduce (or the previous part) ended with a barrier
+            {
+                constexpr int SU = 4;
+                __syncthreads();
+                for (int k0 = threadIdx.x; k0 < nh; k0 += SU * NT) {
+                    double a[SU], c[SU], e[SU], d[SU];
+#pragma unroll
+                    for (int u = 0; u < SU; ++u) {
+                        const int k = k0 + u * NT;
+                        const int j = k < nh ? D.halo_idx[h0 + k] : 0;
+                        a[u] = __ldcg(so + j);
+                        c[u] = __ldcg(wo + j);
+                        e[u] = __ldcg(ro + j);
+                        d[u] = dzres ? 0.0 : __ldcg(dz + j);
+                    }
+#pragma unroll
+                    for (int u = 0; u < SU; ++u) {
+                        const int k = k0 + u * NT;
+                        if (k < nh) {
+                            const double sj = fma(beta, a[u], c[u]);
+                            const double rj = fma(-alpha, sj, e[u]);
+                            vh[k] = rj * (dzres ? dzh[k] : d[u]);
+                        }
+                    }
+                }
+                __syncthreads();
+            }
+            // own rows: p = z_o + beta*p, s = w_o + beta*s_o, x += alpha*p,
+            // r = r_o - alpha*s; then w = A z, the partials
+            for (int s = ps0 + warp; s < ps1; s += PCG_WARPS) {
+                const int i = s * 32 + lane;
+                const uint8_t f = D.nflag[i];
+                const bool fr = (f & 1) && !(f & 4);
+                const double r_o = ro[i], s_o = so[i], w_o = wo[i], dd = dz[i];
+                const double p_o = pv[i];
+                const double off = offdiag(s);
+                const double zo = r_o * dd;
+                const double pi = fr ? fma(beta, p_o, zo) : 0.0;
+                const double si = fma(beta, s_o, w_o);
+                if (fr) D.pres[i] = fma(alpha, pi, D.pres[i]);
+                const double ri = fma(-alpha, si, r_o);
+                pv[i] = pi;
+                rb[pn][i] = ri;
+                sb[pn][i] = si;
+                const double zi = ri * dd;
+                const double wi = fr ? fma(D.pdiag[i], zi, off) : 0.0;
+                wb[pn][i] = wi;
+                if (fr) {
+                    if (!isfinite(ri)) a6.flag = 1.0;
+                    a6.a = fma(ri, zi, a6.a);
+                    a6.b = fma(zi, wi, a6.b);
+                    a6.c = fma(ri, ri, a6.c);
+                    a6.mx = fmax(a6.mx, fabs(ri));
+                }
+            }
+        }
+        t = Acc6{0.0, 0.0, 0.0, 0.0, 0.0};
+        if (!grid_allreduce3<NT>(a6, D, g, phase, t)) return;
+        ++phase;
+        fin = sqrt(t.c);
+        mx = t.mx;
+        rel = fin / init;
+        if (cg_converged(g.conv_test, rel, mx, g.rel_tol, g.abs_tol)) { conv = 1; break; }
+        if (t.flag > 0.0) { if (b == 0 && threadIdx.x == 0) set_status(seg_status(D, g), 4, ST_PCG, it, R_PCG_RESID); return; }
+        const double gn = t.a;
+        if (gn <= 1.0e-300 || !isfinite(gn)) { if (b == 0 && threadIdx.x == 0) set_status(seg_status(D, g), 3, ST_PCG, it, R_PCG_RZ); return; }
+        beta = gn / gam;
+        den = t.b - beta * gn / alpha;
+        gam = gn;
+    }
+    if (it > g.max_iter) it = g.max_iter;
+    cg_finish(D, g, it, conv, init, fin, rel, mx);
+    if (!conv && b == 0 && threadIdx.x == 0) set_status(seg_status(D, g), 2, ST_PCG, it, R_PCG_MAXIT);
+}
+
 template <int RMAX, bool BATCH, int NT, int KS = 0>
 __global__ void __launch_bounds__(NT, NT >= 512 ? 1 : 2) k_pcg64c(PcgDev D)
 {
@@ -2521,7 +2766,7 @@ void PcgEngine::init(const HostModel& m, const uint8_t* nflag, const double* pfi
             }
         }
     }
-    if (variant == 1 && kernel_choice != 1) {
+    if (variant == 1 && kernel_choice != 1 && kernel_choice != 5) {
         const void* cands[4] = {reinterpret_cast<const void*>(k_pcg64r<1>), reinterpret_cast<const void*>(k_pcg64r<2>),
                                 reinterpret_cast<const void*>(k_pcg64r<4>), reinterpret_cast<const void*>(k_pcg64r<8>)};
         for (int c = 0; c < 4; ++c) {
@@ -2565,7 +2810,10 @@ void PcgEngine::init(const HostModel& m, const uint8_t* nflag, const double* pfi
             }
             if (fits) global_halo_parts = kp;
         }
-        const void* fh = reinterpret_cast<const void*>(k_pcg64<true>);
+        // automatic and choice 5: the single-reduction kernel; choice 1:
+        // the two-reduction one (bitwise the same arithmetic as choices 2, 3)
+        global_cgcg = kernel_choice != 1;
+        const void* fh = global_cgcg ? reinterpret_cast<const void*>(k_pcg64g) : reinterpret_cast<const void*>(k_pcg64<true>);
         const size_t smem = static_cast<size_t>(hmax) * 16 + 16;
         int per = 0;
         if (fits && raise_smem_limit(fh, smem) == cudaSuccess &&
@@ -2709,7 +2957,9 @@ cbs3d_status PcgEngine::solve(double* pres, double* rhs1, double* pdiag, int pre
     CUDA_OK(cudaMemsetAsync(d_bar, 0, 4 * sizeof(unsigned), st));
     CUDA_OK(cudaMemsetAsync(d_out, 0, sizeof(CgOut), st));
     void* args[] = {&D};
-    const void* fn = global_halo ? reinterpret_cast<const void*>(k_pcg64<true>) : reinterpret_cast<const void*>(k_pcg64<false>);
+    const void* fn = !global_halo ? reinterpret_cast<const void*>(k_pcg64<false>)
+                     : global_cgcg ? reinterpret_cast<const void*>(k_pcg64g)
+                                   : reinterpret_cast<const void*>(k_pcg64<true>);
     size_t smem = global_halo ? global_halo_smem : 0;
     if (variant == 2) {
         if (rmax == 1) fn = reinterpret_cast<const void*>(k_pcg64r<1>);
@@ -2816,6 +3066,15 @@ size_t PcgEngine::bytes_per_iter() const
     // Phase B: q, r, pres, pdiag read (32), r, pres, z written (24).  With the
     // shared-memory halo the columns are 16-bit and every halo entry's z and
     // previous p are read once per iteration.
+    if (global_halo && global_cgcg) {
+        // single reduction: coefficient + 16-bit column per pair entry; per
+        // node r, s, w of the previous iteration, p, pressure, inverse
+        // diagonal and diagonal read (56), node flag (1), p, pressure and the
+        // new r, s, w written (40); per halo entry r, s, w (24) and, with
+        // several parts per CTA, the inverse diagonal (8)
+        return static_cast<size_t>(nnz_offdiag) * 10 + static_cast<size_t>(N) * 97 +
+               static_cast<size_t>(global_halo_total) * (global_halo_parts > 1 ? 32 : 24);
+    }
     if (global_halo)
         return static_cast<size_t>(nnz_offdiag) * 10 + static_cast<size_t>(N) * 97 +
                static_cast<size_t>(global_halo_total) * 16;

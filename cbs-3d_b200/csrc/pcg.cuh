@@ -82,9 +82,10 @@ struct CoarseDev {
 // Owns the device copies of the pattern and the PCG work vectors.
 class PcgEngine {
 public:
-    // kernel_choice: 0 automatic (4, else 3, else 2, else 1), 1 vectors in global memory,
+    // kernel_choice: 0 automatic (4, else 3, else 2, else 5), 1 vectors in global memory,
     // 2 register-resident rows, 3 with the halo staged in shared memory,
-    // 4 as 3 with one grid synchronisation per iteration (Chronopoulos-Gear)
+    // 4 as 3 with one grid synchronisation per iteration (Chronopoulos-Gear),
+    // 5 vectors in global memory with one grid synchronisation per iteration
     // two_level: Jacobi plus a coarse correction on one aggregate per CTA
     // (large meshes with the single-reduction kernel; else plain Jacobi)
     // multigrid: the aggregation-multigrid preconditioned CG (mg.cuh) for
@@ -130,6 +131,7 @@ public:
     void coarse_setup(const double* pdiag, const int* row_node, cudaStream_t st);
     int variant = 1;         // 1 global vectors, 2 register rows, 3 + shared-memory halo, 4 + one sync per iteration
     bool global_halo = false;     // variant 1 with its neighbour values staged in shared memory
+    bool global_cgcg = false;     // ... run by the single-reduction kernel k_pcg64g
     size_t global_halo_smem = 0;
     long long global_halo_total = 0;   // halo entries over all CTAs
     int global_halo_parts = 1;         // parts per CTA, each with its own halo

@@ -97,7 +97,8 @@ typedef struct cbs3d_options {
     int verbose;
     int time_pcg;            /* time every PCG launch with CUDA events (no graph capture) */
     int pcg_kernel;          /* 0 automatic; 1 vectors in global memory, 2 register-resident rows,
-                                3 shared-memory halo, 4 halo + one grid sync per iteration */
+                                3 shared-memory halo, 4 halo + one grid sync per iteration,
+                                5 vectors in global memory + one grid sync per iteration */
     int case_cache;          /* cbs3d_create_from_case: keep the parsed case in <case>.cbscache
                                 (keyed by every source file's size and time) and reuse it */
     int pcg_two_level;       /* extension: Jacobi plus a coarse correction on one aggregate of rows
@@ -142,7 +143,8 @@ typedef struct cbs3d_step_stats {
     int pcg_kernel;          /* PCG kernel in use: 1 global vectors, 2 register rows,
                                 3 shared-memory halo, 4 single-reduction (CG-CG),
                                 5 mixed FP32/FP64, 6 two-level (CG-CG + coarse correction),
-                                7 aggregation-multigrid preconditioned CG */
+                                7 aggregation-multigrid preconditioned CG,
+                                8 global vectors, single-reduction (CG-CG) */
 } cbs3d_step_stats;
 
 typedef struct cbs3d_ctx cbs3d_ctx;
