@@ -14,11 +14,17 @@ def _gpu():
     return gpu
 
 
-def test_not_converged_reports_and_context_survives():
+# every PCG kernel checks the same conditions: automatic, the two global-vector
+# kernels (two reductions, single reduction) and the register single-reduction one
+KERNELS = [0, 1, 4, 5]
+
+
+@pytest.mark.parametrize("kernel", KERNELS)
+def test_not_converged_reports_and_context_survives(kernel):
     case, _ = load_case(fixture_path("cav6j"))
     case.params["cg_max_iter"] = 2
     gpu = _gpu()
-    c = gpu.Context(case)
+    c = gpu.Context(case, pcg_kernel=kernel)
     with pytest.raises(gpu.CBSError) as e:
         c.step(1)
     assert e.value.code == 2
@@ -27,10 +33,11 @@ def test_not_converged_reports_and_context_survives():
     assert np.all(np.isfinite(u))
 
 
-def test_nonfinite_velocity_is_reported():
+@pytest.mark.parametrize("kernel", KERNELS)
+def test_nonfinite_velocity_is_reported(kernel):
     case, _ = load_case(fixture_path("cav6j"))
     gpu = _gpu()
-    c = gpu.Context(case)
+    c = gpu.Context(case, pcg_kernel=kernel)
     u, p, t = c.fields()
     interior = 3 * 150
     u[interior] = np.nan
