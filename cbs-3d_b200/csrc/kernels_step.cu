@@ -224,12 +224,17 @@ __global__ void k_timestep(DevState S, int fixed_dt)
                 u /= 4.0; v /= 4.0; w /= 4.0;
                 speed = sqrt(u * u + v * v + w * w);
             } else {
-                speed = 0.0;
+                // max_a sqrt(|u_a|^2) as sqrt(max_a |u_a|^2): the square root
+                // is correctly rounded, hence monotonic, so the two are equal
+                // bit for bit (a NaN is skipped by std::max either way)
+                double m = 0.0;
+#pragma unroll
                 for (int a = 0; a < 4; ++a) {
                     const int ip = node_of(n, a);
                     const double u = S.unkno[3 * ip], v = S.unkno[3 * ip + 1], w = S.unkno[3 * ip + 2];
-                    speed = dmax(speed, sqrt(u * u + v * v + w * w));
+                    m = dmax(m, u * u + v * v + w * w);
                 }
+                speed = sqrt(m);
             }
             double diff = S.P.ani;
             const bool fluid = S.mat[e] == 0;
