@@ -34,7 +34,9 @@ over a 48 MiB buffer in one launch, cbs3d_probe_bandwidth; the PCG's L2
 traffic is almost all reads), with the grid
 all-reduce latency (cbs3d_probe_allreduce) as the per-iteration floor;
 "hbm_case" runs the same FP64 engine on a 96^3 cavity, whose per-iteration
-traffic exceeds L2, against the measured HBM copy bandwidth.
+traffic exceeds L2 (the single-reduction global-vector kernel k_pcg64g),
+against the HBM figure of MEASURED_PEAKS.json, else the 6,650 GB/s fallback
+measured earlier on this pool (its source is stated in the line).
 
 Multi-GPU: the single-case path does not shard (replicas only); each rank
 runs its own replica and `value` is the total steps/s of all ranks.
@@ -151,8 +153,8 @@ def measured_peak():
 
 
 def probes(device: int) -> dict:
-    """L2 and HBM copy bandwidth and the grid all-reduce latency on this GPU,
-    measured with the library's probe kernels (CUDA events)."""
+    """L2 and HBM read and copy bandwidths and the grid all-reduce latency on
+    this GPU, measured with the library's probe kernels (CUDA events)."""
     import ctypes
 
     from cbs3d import gpu
@@ -299,9 +301,9 @@ def timed_run(args, ctx, dist):
 
 def roofline(st, warm, nelem_fluid, npoin, mixed, n, pr, bound="l2"):
     """PCG kernel roofline: the kernel's own bytes per iteration over its
-    CUDA-event time, against the L2 copy bandwidth measured in this run
-    (bound "l2": the solve's operator and vectors stay in L2) or the
-    measured HBM copy bandwidth (bound "hbm")."""
+    CUDA-event time, against the L2 read bandwidth measured in this run
+    (bound "l2": the solve's operator and vectors stay in L2) or the HBM
+    figure (bound "hbm": MEASURED_PEAKS.json, else the fallback)."""
     hbm, hbm_kind = measured_peak()
     its = st.cg_iterations_total - warm.cg_iterations_total   # totals are cumulative
     kb = float(st.pcg_bytes_per_iter)
