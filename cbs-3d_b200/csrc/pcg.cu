@@ -1274,6 +1274,10 @@ __global__ void __launch_bounds__(NT, NT >= 512 ? 1 : 2) k_pcg64c(PcgDev D)
     constexpr bool XS = NT == 256 && !BATCH;
     double* xs = XS && D.xs_off ? reinterpret_cast<double*>(smem_raw + D.xs_off) : nullptr;
     double* pds = xs ? xs + RMAX * NT : nullptr;
+    // XR: the own rows' pressure held in registers for the solve and stored
+    // on every exit (the one-CTA-per-SM kernel: 12.18 -> 11.73 us per
+    // iteration at 64^3; holding the diagonal there too was slower, 14.0 us)
+    constexpr bool XR = NT == 512 && !BATCH;
     for (int k = threadIdx.x; k < nh; k += NT) hidx[k] = D.halo_idx[h0 + k];
     for (int k = threadIdx.x; k < nsl; k += NT) lcs[k] = D.lcol[S0 + k];
     // KS = 1: the coefficients of every warp's first row (the CTA's first
@@ -1294,6 +1298,7 @@ __global__ void __launch_bounds__(NT, NT >= 512 ? 1 : 2) k_pcg64c(PcgDev D)
     double* dz = D.z;   // free ? 1/diagonal : 0  (z = r * dz)
 
     double r[RMAX], p[RMAX], s[RMAX], w[RMAX], dd[RMAX];
+    double xr[RMAX];
     bool fr[RMAX];
     int row[RMAX], lbase[RMAX], wr[RMAX];
     int wmax = 0;
@@ -1309,6 +1314,7 @@ __global__ void __launch_bounds__(NT, NT >= 512 ? 1 : 2) k_pcg64c(PcgDev D)
             wmax = wr[k] > wmax ? wr[k] : wmax;
         }
         r[k] = p[k] = s[k] = w[k] = 0.0;
+        xr[k] = 0.0;
         dd[k] = 0.0;   // reciprocal of the Jacobi diagonal; 0 off the free rows
         fr[k] = false;
     }
@@ -1367,6 +1373,7 @@ __global__ void __launch_bounds__(NT, NT >= 512 ? 1 : 2) k_pcg64c(PcgDev D)
             xs[k * NT + threadIdx.x] = xi;
             pds[k * NT + threadIdx.x] = pd;
         }
+        if (XR) xr[k] = xi;
         const double y = fma(pd, xi, off[k]);
         double ri = active ? D.rhs1[i] - y : 0.0;
         if (!fr[k]) ri = 0.0;
@@ -1388,6 +1395,12 @@ __global__ void __launch_bounds__(NT, NT >= 512 ? 1 : 2) k_pcg64c(PcgDev D)
     }
     // the pressure of the free own rows back to global memory
     auto store_x = [&]() {
+        if (XR) {
+#pragma unroll
+            for (int k = 0; k < RMAX; ++k)
+                if (row[k] >= 0 && fr[k]) D.pres[row[k]] = xr[k];
+            return;
+        }
         if (!xs) return;
 #pragma unroll
         for (int k = 0; k < RMAX; ++k)
@@ -1485,7 +1498,8 @@ __global__ void __launch_bounds__(NT, NT >= 512 ? 1 : 2) k_pcg64c(PcgDev D)
             p[k] = fr[k] ? fma(beta, p[k], zo) : 0.0;
             s[k] = fma(beta, s[k], w[k]);
             if (fr[k]) {
-                if (xs) xs[k * NT + threadIdx.x] = fma(alpha, p[k], xs[k * NT + threadIdx.x]);
+                if (XR) xr[k] = fma(alpha, p[k], xr[k]);
+                else if (xs) xs[k * NT + threadIdx.x] = fma(alpha, p[k], xs[k * NT + threadIdx.x]);
                 else D.pres[i] = fma(alpha, p[k], D.pres[i]);
             }
             r[k] = fma(-alpha, s[k], r[k]);
