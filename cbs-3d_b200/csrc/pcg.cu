@@ -1273,7 +1273,8 @@ __global__ void __launch_bounds__(NT, NT >= 512 ? 1 : 2) k_pcg64c(PcgDev D)
     // meshes only; the other instantiations compile the global accesses alone)
     constexpr bool XS = NT == 256 && !BATCH;
     double* xs = XS && D.xs_off ? reinterpret_cast<double*>(smem_raw + D.xs_off) : nullptr;
-    double* pds = xs ? xs + RMAX * NT : nullptr;
+    double* pds = xs ? xs + RMAX * NT
+                : (NT == 512 && !BATCH && D.pds_off ? reinterpret_cast<double*>(smem_raw + D.pds_off) : nullptr);
     // XR: the own rows' pressure held in registers for the solve and stored
     // on every exit (the one-CTA-per-SM kernel: 12.18 -> 11.73 us per
     // iteration at 64^3; holding the diagonal there too was slower, 14.0 us)
@@ -1369,10 +1370,8 @@ __global__ void __launch_bounds__(NT, NT >= 512 ? 1 : 2) k_pcg64c(PcgDev D)
         fr[k] = (f & 1) && !(f & 4);
         const double pd = D.pdiag[i];
         const double xi = D.pres[i];
-        if (xs) {
-            xs[k * NT + threadIdx.x] = xi;
-            pds[k * NT + threadIdx.x] = pd;
-        }
+        if (xs) xs[k * NT + threadIdx.x] = xi;
+        if (pds) pds[k * NT + threadIdx.x] = pd;
         if (XR) xr[k] = xi;
         const double y = fma(pd, xi, off[k]);
         double ri = active ? D.rhs1[i] - y : 0.0;
@@ -1440,7 +1439,7 @@ __global__ void __launch_bounds__(NT, NT >= 512 ? 1 : 2) k_pcg64c(PcgDev D)
         const int i = row[k];
         if (i < 0) continue;
         const double zi = r[k] * dd[k];
-        w[k] = fr[k] ? fma(xs ? pds[k * NT + threadIdx.x] : D.pdiag[i], zi, off[k]) : 0.0;
+        w[k] = fr[k] ? fma(pds ? pds[k * NT + threadIdx.x] : D.pdiag[i], zi, off[k]) : 0.0;
         wb[0][i] = w[k];
         if (fr[k]) {
             acc.a = fma(r[k], zi, acc.a);
@@ -1513,7 +1512,7 @@ __global__ void __launch_bounds__(NT, NT >= 512 ? 1 : 2) k_pcg64c(PcgDev D)
             const int i = row[k];
             if (i < 0) continue;
             const double zi = r[k] * dd[k];
-            w[k] = fr[k] ? fma(xs ? pds[k * NT + threadIdx.x] : D.pdiag[i], zi, off[k]) : 0.0;
+            w[k] = fr[k] ? fma(pds ? pds[k * NT + threadIdx.x] : D.pdiag[i], zi, off[k]) : 0.0;
             wb[pn][i] = w[k];
             if (fr[k]) {
                 if (!isfinite(r[k])) a6.flag = 1.0;
@@ -2754,6 +2753,23 @@ void PcgEngine::init(const HostModel& m, const uint8_t* nflag, const double* pfi
                 }
                 cudaGetLastError();
             }
+            // the one-CTA-per-SM kernel's rows' diagonal in shared memory
+            // (64^3: 12.05 -> 11.95 us per iteration; in registers it was
+            // slower)
+            cgcg_pds_off = 0;
+            if (want == 4 && nt == 512) {
+                const size_t off = (cgcg_smem + 15) & ~static_cast<size_t>(15);
+                const size_t with = off + static_cast<size_t>(rm[c]) * nt * 8;
+                const void* fk = fn_cgcg_single(rm[c], nt, cgcg_ks);
+                int per2 = 0;
+                if (with <= 227 * 1024 && raise_smem_limit(fk, with) == cudaSuccess &&
+                    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per2, fk, nt, with) == cudaSuccess &&
+                    per2 * sms >= g) {
+                    cgcg_smem = with;
+                    cgcg_pds_off = static_cast<int>(off);
+                }
+                cudaGetLastError();
+            }
             d_halo_ptr = dalloc<int>(hptr.size());
             d_halo_idx = dalloc<int>(hidx.size());
             d_lcol = dalloc<unsigned short>(lcol.size());
@@ -2886,6 +2902,7 @@ void PcgEngine::init(const HostModel& m, const uint8_t* nflag, const double* pfi
     dev.halo_ptr = d_halo_ptr; dev.halo_idx = d_halo_idx; dev.lcol = d_lcol; dev.halo_max = dev_halo_max;
     dev.xs_off = cgcg_xs_off;
     dev.coef_off = cgcg_coef_off;
+    dev.pds_off = cgcg_pds_off;
     dev.halo_parts = global_halo ? global_halo_parts : 0;
     dev.row_node = d_row_node;
 }

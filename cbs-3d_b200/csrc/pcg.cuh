@@ -62,6 +62,8 @@ struct PcgDev {
                                  // with its own halo (halo_ptr indexed by CTA*parts + part)
     int coef_off;                // CG-CG kernel with its warps' first rows' coefficients in shared
                                  // memory: byte offset of that copy
+    int pds_off;                 // one-CTA-per-SM CG-CG kernel: byte offset in shared memory of its
+                                 // rows' diagonal (RMAX*threads doubles); 0: read from global memory
 };
 
 class MgHierarchy;
@@ -140,6 +142,7 @@ public:
     int cgcg_xs_off = 0;     // where those rows start (0: kept in global memory)
     int cgcg_ks = 0;         // 1: the kernel reads its warps' first rows' coefficients from shared memory
     int cgcg_coef_off = 0;   // where they start
+    int cgcg_pds_off = 0;    // where the rows' diagonal starts in shared memory (0: global memory)
     size_t mixed_smem = 0;   // dynamic shared memory of the mixed-precision kernel
     bool mixed_ok = false;   // mixed precision runs on the FP32 kernel (else FP64)
     int dev_slot_max = 0;
