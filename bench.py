@@ -206,12 +206,13 @@ def cpu_baseline(n: int) -> dict:
     if not os.path.exists(reference_harness()):
         return {"value": None, "unit": "steps/s", "cores": threads, "kind": "reference",
                 "sample": "unavailable: oracle/_ref/cbs_ref_harness not built"}
-    case = make_case(n, ntime=2)
-    r = run_reference(case, steps=1, warmup=0, threads=threads)
+    # the first three CBS steps (about 12 s on 16 host cores at 64^3)
+    case = make_case(n, ntime=4)
+    r = run_reference(case, steps=3, warmup=0, threads=threads)
     return {"value": r["steps_per_s"], "unit": "steps/s", "cores": r["threads"], "kind": "reference",
-            "sample": f"first CBS step of the same {n}^3 cavity ({r['last_cg_iterations']} PCG iterations), "
-                      f"reference compiled from its sources, OpenMP {r['threads']} threads, "
-                      f"{r['seconds']:.1f} s"}
+            "sample": f"first {r['steps']} CBS steps of the same {n}^3 cavity ({r['last_cg_iterations']} PCG "
+                      f"iterations in the last), reference compiled from its sources, OpenMP {r['threads']} "
+                      f"threads, {r['seconds']:.1f} s"}
 
 
 # ----------------------------------------------------------------- arms
@@ -253,8 +254,10 @@ def arm_reference(args):
         return
     case = make_case(args.n, ntime=10 ** 6)
     threads = os.cpu_count() or 1
-    k = max(1, min(args.steps, 2))
-    w = min(args.warmup, 1)
+    # the requested steps, up to 20 timed after up to 5 warm-up steps (about
+    # 4-5 s each on 16 host cores at 64^3), so the run ends within minutes
+    k = max(1, min(args.steps, 20))
+    w = min(args.warmup, 5)
     if not os.path.exists(reference_harness()):
         print(json.dumps({"impl": "reference", "unavailable": "reference harness oracle/_ref not built"}))
     else:
