@@ -74,6 +74,7 @@ void cbs3d_ctx::setup(bool own_pcg)
     CUDA_OK(cudaStreamCreateWithFlags(&side, cudaStreamNonBlocking));
     CUDA_OK(cudaEventCreateWithFlags(&ev_fork, cudaEventDisableTiming));
     CUDA_OK(cudaEventCreateWithFlags(&ev_join, cudaEventDisableTiming));
+    CUDA_OK(cudaEventCreateWithFlags(&ev_lhs, cudaEventDisableTiming));
     own_engine = own_pcg;
     const size_t E = m.E, N = m.N;
     DevParams& P = S.P;
@@ -239,9 +240,26 @@ void cbs3d_ctx::enqueue_pre(int it)
 {
     k_begin_step<<<nb(m.N), T, 0, st>>>(S);
     stage_time_step(it);
-    k_lhs<<<nb(m.N), T, 0, st>>>(S);
-    if (m.p.step2_check <= 0) fork_assembly();
+    // The Step-1 element kernel reads none of the LHS's outputs (elcoe2,
+    // elcoe2p, pdiag, the constrained rows' p and rhs1), so the LHS runs on
+    // the side stream beside it, followed there by the operator assembly;
+    // the Step-1 node gather, which reads elcoe2, waits for the LHS.
+    const bool lhs_side = m.p.step2_check <= 0 && own_engine;
+    if (lhs_side) {
+        CUDA_OK(cudaEventRecord(ev_fork, st));
+        CUDA_OK(cudaStreamWaitEvent(side, ev_fork, 0));
+        k_lhs<<<nb(m.N), T, 0, side>>>(S);
+        CUDA_OK(cudaEventRecord(ev_lhs, side));
+        pcg.assemble_from_state(S, side);
+        pcg.prepare_coarse(S.pdiag, side);
+        CUDA_OK(cudaEventRecord(ev_join, side));
+        assembly_forked = true;
+    } else {
+        k_lhs<<<nb(m.N), T, 0, st>>>(S);
+        if (m.p.step2_check <= 0) fork_assembly();
+    }
     k_step1_elem<<<nb(m.E, 128), 128, 0, st>>>(S);
+    if (lhs_side) CUDA_OK(cudaStreamWaitEvent(st, ev_lhs, 0));
     k_step1_node<<<nb(m.N), T, 0, st>>>(S);
     if (m.p.step2_check > 0) {
         k_dt_correction<<<nb(m.E), T, 0, st>>>(S);

@@ -74,6 +74,7 @@ struct cbs3d_ctx {
     // onto `side` after the last LHS update so that it overlaps Steps 1-2
     cudaStream_t side = nullptr;
     cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
+    cudaEvent_t ev_lhs = nullptr;      // the LHS on `side`, waited for by the Step-1 node gather
     bool own_engine = false, assembly_forked = false;
     cudaGraphExec_t gexec = nullptr;
     bool graph_failed = false;
@@ -99,6 +100,7 @@ struct cbs3d_ctx {
         if (ev1) cudaEventDestroy(ev1);
         if (ev_fork) cudaEventDestroy(ev_fork);
         if (ev_join) cudaEventDestroy(ev_join);
+        if (ev_lhs) cudaEventDestroy(ev_lhs);
         if (side) cudaStreamDestroy(side);
         if (st) cudaStreamDestroy(st);
     }
