@@ -325,3 +325,22 @@ def test_global_single_reduction_bitwise_equals_register_kernel():
         assert sa.cg.iterations == sb.cg.iterations
     for x, y in zip(a.fields(), b.fields()):
         assert bitwise(x, y)
+
+
+def test_large_mesh_runs_single_reduction_global_kernel():
+    """Beyond the register tiling (88^3 cavity: 704,969 nodes on 148 SMs) the
+    engine runs the single-reduction global-vector kernel by itself; after
+    two steps it agrees with the two-reduction kernel to RUN_TOL, with
+    iteration counts within 2."""
+    from cbs3d import cases
+    gpu = _gpu()
+    case = cases.cavity(88, re=400.0, ntime=10 ** 6, jitter=0.15, seed=1234)
+    a = gpu.Context(case)
+    b = gpu.Context(case, pcg_kernel=1)
+    for _ in range(2):
+        sa, sb = a.step(1), b.step(1)
+        assert sa.pcg_kernel == 8 and sb.pcg_kernel == 1
+        assert abs(sa.cg.iterations - sb.cg.iterations) <= 2
+    (ua, pa, _), (ub, pb, _) = a.fields(), b.fields()
+    assert rel_l2(ua, ub) <= RUN_TOL
+    assert rel_l2(pa, pb) <= RUN_TOL
