@@ -287,7 +287,7 @@ def ebe_bytes(nelem_fluid: int, npoin: int, mixed: bool) -> int:
 
 
 KERNELS = {1: "k_pcg64", 2: "k_pcg64r", 3: "k_pcg64h", 4: "k_pcg64c", 5: "k_pcg32m", 6: "k_pcg64d", 7: "k_pcg_mg",
-           8: "k_pcg64g"}
+           8: "k_pcg64g", 9: "k_pcg64c"}
 
 
 def timed_run(args, ctx, dist):

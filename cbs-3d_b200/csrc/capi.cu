@@ -505,7 +505,8 @@ static DevStatus collect_call(cbs3d_ctx* c, int done, int start, long long launc
     if (!c->batch_out) {
         stats->pcg_bytes_per_iter = static_cast<double>(c->pcg.bytes_per_iter());
         stats->pcg_kernel = c->pcg.mgh ? 7 : c->pcg.coarse ? 6 : c->pcg.variant == 4 && c->pcg.mixed_ok ? 5
-                          : c->pcg.variant == 1 && c->pcg.global_halo && c->pcg.global_cgcg ? 8 : c->pcg.variant;
+                          : c->pcg.variant == 1 && c->pcg.global_halo && c->pcg.global_cgcg ? 8
+                          : c->pcg.variant == 4 && c->pcg.cgcg_kt > 0 ? 9 : c->pcg.variant;
     }
     for (int k = 0; k + 1 < c->pcg_ev_used; k += 2) {
         float pm = 0.0f;

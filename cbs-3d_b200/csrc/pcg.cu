@@ -880,17 +880,28 @@ __device__ __forceinline__ bool grid_allreduce_v(double (&v)[NV], const PcgDev& 
             const double x = __shfl_down_sync(0xffffffffu, t[q], o);
             t[q] = q < NSUM ? t[q] + x : fmax(t[q], x);
         }
-    __syncthreads();
+    // sm was last read by thread 0 before the barrier that published s_ok,
+    // so the warps' totals can overwrite it now.  Thread q folds value q
+    // over the warps in warp order (the same sums as every thread folding
+    // all of them) and the warps read the NV results: NV shared-memory
+    // reads per warp instead of NV * warps broadcasts, which at 16 warps
+    // kept the shared-memory pipe busy for ~1,300 cycles per all-reduce.
+    __shared__ double so[NV];
     if (lane == 0)
 #pragma unroll
         for (int q = 0; q < NV; ++q) sm[w][q] = t[q];
     __syncthreads();
-#pragma unroll
-    for (int q = 0; q < NV; ++q) out[q] = 0.0;
-    for (int k = 0; k < (NT / 32); ++k)
-#pragma unroll
-        for (int q = 0; q < NV; ++q) out[q] = q < NSUM ? out[q] + sm[k][q] : fmax(out[q], sm[k][q]);
+    if (threadIdx.x < NV) {
+        const int q = threadIdx.x;
+        double x = 0.0;
+        for (int k = 0; k < (NT / 32); ++k) x = q < NSUM ? x + sm[k][q] : fmax(x, sm[k][q]);
+        so[q] = x;
+    }
     __syncthreads();
+    // no barrier after these reads: so is rewritten only after the next
+    // call's second barrier, which every thread reaches after reading it
+#pragma unroll
+    for (int q = 0; q < NV; ++q) out[q] = so[q];
     return ok;
 }
 
@@ -1251,8 +1262,72 @@ __global__ void __launch_bounds__(PCG_THREADS, PCG_CTAS_PER_SM) k_pcg64g(PcgDev 
     if (!conv && b == 0 && threadIdx.x == 0) set_status(seg_status(D, g), 2, ST_PCG, it, R_PCG_MAXIT);
 }
 
-template <int RMAX, bool BATCH, int NT, int KS = 0>
-__global__ void __launch_bounds__(NT, NT >= 512 ? 1 : 2) k_pcg64c(PcgDev D)
+// ---------------------------------------------- tensor memory as storage
+// The SM's 256 KB tensor memory (TMEM: 128 lanes x 512 columns of 32 bits)
+// holds, for the whole solve, coefficients that would otherwise stream from
+// L2 in every iteration.  No MMA touches it: it is read with tcgen05.ld into
+// registers.  With the 32x32b access shape, warp w reads and writes lanes
+// 32*(w%4) .. 32*(w%4)+31, one lane per thread, so the four warps that share
+// a lane quarter split the 512 columns into four ranges of 128.  One warp
+// allocates all 512 columns (one CTA per SM, nothing else in this library
+// uses TMEM) and frees them before the CTA exits, on every path.
+__device__ __forceinline__ void tmem_alloc_all(uint32_t* slot)
+{
+    const uint32_t a = static_cast<uint32_t>(__cvta_generic_to_shared(slot));
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], 512;" ::"r"(a) : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+}
+__device__ __forceinline__ void tmem_free_all(uint32_t base)
+{
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, 512;" ::"r"(base) : "memory");
+}
+__device__ __forceinline__ void tmem_fence_before_sync() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void tmem_fence_after_sync() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+// one double into two consecutive columns of this thread's lane (low word first)
+__device__ __forceinline__ void tmem_st_f64(uint32_t addr, double v)
+{
+    const unsigned long long b = static_cast<unsigned long long>(__double_as_longlong(v));
+    asm volatile("tcgen05.st.sync.aligned.32x32b.x2.b32 [%0], {%1, %2};" ::"r"(addr),
+                 "r"(static_cast<uint32_t>(b)), "r"(static_cast<uint32_t>(b >> 32))
+                 : "memory");
+}
+__device__ __forceinline__ void tmem_wait_st() { asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory"); }
+// N consecutive 32-bit columns of this thread's lane; the registers are
+// undefined until tmem_wait_ld, after which tmem_hold pins their uses
+template <int N>
+__device__ __forceinline__ void tmem_ld(uint32_t addr, uint32_t (&r)[N]);
+template <>
+__device__ __forceinline__ void tmem_ld<4>(uint32_t addr, uint32_t (&r)[4])
+{
+    asm volatile("tcgen05.ld.sync.aligned.32x32b.x4.b32 {%0, %1, %2, %3}, [%4];"
+                 : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3])
+                 : "r"(addr));
+}
+template <>
+__device__ __forceinline__ void tmem_ld<16>(uint32_t addr, uint32_t (&r)[16])
+{
+    asm volatile("tcgen05.ld.sync.aligned.32x32b.x16.b32 "
+                 "{%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15}, [%16];"
+                 : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
+                   "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]),
+                   "=r"(r[14]), "=r"(r[15])
+                 : "r"(addr));
+}
+__device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
+// after tmem_wait_ld: an empty statement that "rewrites" the loaded registers,
+// so no use of them can be scheduled before the wait
+template <int N>
+__device__ __forceinline__ void tmem_hold(uint32_t (&r)[N])
+{
+#pragma unroll
+    for (int i = 0; i < N; ++i) asm volatile("" : "+r"(r[i]));
+}
+
+// KT > 0: the coefficients of each thread's rows KS .. KS+KT-1 live in TMEM
+// for the solve (D.tm_w slots per row, zero-padded past the slice's width);
+// `tm` is the CTA's TMEM base address (0 when KT = 0).
+template <int RMAX, bool BATCH, int NT, int KS, int KT>
+__device__ __forceinline__ void pcg64c_body(const PcgDev& D, uint32_t tm)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const SegView g = seg_view<BATCH>(D);
@@ -1322,18 +1397,58 @@ __global__ void __launch_bounds__(NT, NT >= 512 ? 1 : 2) k_pcg64c(PcgDev D)
     // coefficient columns loaded per round (measured: 2 rather than 4 at four
     // rows per thread takes the 64^3 iteration from 13.0 to 12.2 us)
     constexpr int CH = (RMAX >= 8) ? 2 : (RMAX >= 4) ? 2 : 8;
+    static_assert(KT == 0 || KS + KT <= RMAX, "TMEM rows follow the shared-memory rows");
+    // TMEM rows: row KS+q of this thread starts at column
+    // 128*(warp/4) + 2*tm_w*q of lane 32*(warp%4)+lane; slot u of the row is
+    // the double in columns 2u, 2u+1.  Every warp runs the same (uniform)
+    // loops here, as the .sync.aligned forms require.
+    uint32_t tmr[KT > 0 ? KT : 1];
+    if constexpr (KT > 0) {
+        const int tw = D.tm_w;
+        const uint32_t wb0 = tm + (static_cast<uint32_t>(32 * (warp & 3)) << 16) + static_cast<uint32_t>(128 * (warp >> 2));
+#pragma unroll
+        for (int q = 0; q < KT; ++q) {
+            tmr[q] = wb0 + static_cast<uint32_t>(2 * tw * q);
+            const int k = KS + q;
+            for (int u = 0; u < tw; ++u) {
+                const double c = (u < wr[k]) ? __ldcg(D.val + S0 + lbase[k] + 32 * u) : 0.0;
+                tmem_st_f64(tmr[q] + 2 * u, c);
+            }
+        }
+        tmem_wait_st();
+    }
     auto offdiag_all = [&](double* off) {
 #pragma unroll
         for (int k = 0; k < RMAX; ++k) off[k] = 0.0;
         for (int k0 = 0; k0 < wmax; k0 += CH) {
             double v[RMAX][CH];
+            uint32_t tv[KT > 0 ? KT : 1][2 * CH];
+            if constexpr (KT > 0) {
 #pragma unroll
-            for (int k = 0; k < RMAX; ++k)
+                for (int q = 0; q < KT; ++q) tmem_ld<2 * CH>(tmr[q] + 2 * k0, tv[q]);
+            }
+#pragma unroll
+            for (int k = 0; k < RMAX; ++k) {
+                if (k >= KS && k < KS + KT) continue;
 #pragma unroll
                 for (int u = 0; u < CH; ++u)
                     v[k][u] = (k0 + u < wr[k]) ? (k < KS ? cvs[lbase[k] + 32 * (k0 + u)]
                                                          : __ldcg(D.val + S0 + lbase[k] + 32 * (k0 + u)))
                                                : 0.0;
+            }
+            if constexpr (KT > 0) {
+                tmem_wait_ld();
+#pragma unroll
+                for (int q = 0; q < KT; ++q) {
+                    tmem_hold<2 * CH>(tv[q]);
+#pragma unroll
+                    for (int u = 0; u < CH; ++u)
+                        v[KS + q][u] = (k0 + u < wr[KS + q])
+                                           ? __hiloint2double(static_cast<int>(tv[q][2 * u + 1]),
+                                                              static_cast<int>(tv[q][2 * u]))
+                                           : 0.0;
+                }
+            }
 #pragma unroll
             for (int k = 0; k < RMAX; ++k)
 #pragma unroll
@@ -1549,6 +1664,33 @@ __global__ void __launch_bounds__(NT, NT >= 512 ? 1 : 2) k_pcg64c(PcgDev D)
     if (it > g.max_iter) it = g.max_iter;
     cg_finish(D, g, it, conv, init, fin, rel, mx);
     if (!conv && b == 0 && threadIdx.x == 0) set_status(seg_status(D, g), 2, ST_PCG, it, R_PCG_MAXIT);
+}
+
+// The single-reduction (Chronopoulos-Gear) Jacobi-PCG with its rows in
+// registers.  KT > 0 (one 512-thread CTA per SM): warp 0 takes the SM's
+// tensor memory before the solve and returns it after; every exit of the
+// body (converged, an error status, a timed-out wait) is CTA-uniform and
+// comes back here, so the memory is freed on every path.
+template <int RMAX, bool BATCH, int NT, int KS = 0, int KT = 0>
+__global__ void __launch_bounds__(NT, NT >= 512 ? 1 : 2) k_pcg64c(PcgDev D)
+{
+    if constexpr (KT == 0) {
+        pcg64c_body<RMAX, BATCH, NT, KS, 0>(D, 0u);
+    } else {
+        static_assert(NT == 512 && !BATCH, "TMEM rows: one CTA per SM, single system");
+        __shared__ uint32_t s_tm;
+        const bool w0 = (threadIdx.x >> 5) == 0;
+        if (w0) tmem_alloc_all(&s_tm);
+        tmem_fence_before_sync();
+        __syncthreads();
+        tmem_fence_after_sync();
+        const uint32_t tm = s_tm;
+        pcg64c_body<RMAX, BATCH, NT, KS, KT>(D, tm);
+        tmem_fence_before_sync();
+        __syncthreads();
+        tmem_fence_after_sync();
+        if (w0) tmem_free_all(tm);
+    }
 }
 
 template <int RMAX>
@@ -2441,6 +2583,70 @@ cbs3d_status coarse_inverse(int device, int g, const double* a, double* ainv, in
 // ============================================================ PcgEngine
 namespace {
 
+// Placement of one CTA's halo in shared memory.  A warp's neighbour gather
+// reads 32 doubles of the halo per slot (one per row of the slice); a double
+// at halo position h sits in the bank pair h mod 16, and two lanes of a half
+// warp whose values share a bank pair without sharing the value cost an
+// extra shared-memory wavefront.  The order of the halo changes no value and
+// no sum, so within every aligned block of 32 positions the block's entries
+// (32 consecutive columns) are placed greedily: entries that occur in the
+// most half-warp gathers first, each at the free position of the block
+// whose bank pair has the fewest entries already placed in those gathers
+// (weighted quadratically).  A block keeps its 32 entries, so the staging
+// loads of each warp touch the same L2 sectors as in column order (a global
+// bank placement spread them over 2.5x the sectors and made the 64^3
+// iteration 17% slower).  64^3 jittered cavity, 148 CTAs: half-warp
+// wavefronts of the gathers 666,745 -> 485,378 per iteration (ideal
+// 391,104).  lc: the slots' halo indices (column order) of slices
+// sb..se-1, offset by a0; returns pos, the position of each entry.
+void bank_spread_halo(int nh, const unsigned short* lc, const long long* slice_off, const int* slice_w, int sb,
+                      int se, long long a0, std::vector<int>& pos)
+{
+    std::vector<std::vector<int>> in_grp(static_cast<size_t>(nh));
+    int ng = 0;
+    for (int s = sb; s < se; ++s)
+        for (int u = 0; u < slice_w[s]; ++u)
+            for (int hw = 0; hw < 2; ++hw, ++ng)
+                for (int l = 16 * hw; l < 16 * hw + 16; ++l) {
+                    auto& v = in_grp[lc[slice_off[s] - a0 + 32 * u + l]];
+                    if (v.empty() || v.back() != ng) v.push_back(ng);
+                }
+    std::vector<unsigned char> cnt(static_cast<size_t>(ng) * 16, 0);
+    pos.assign(static_cast<size_t>(nh), 0);
+    for (int b0 = 0; b0 < nh; b0 += 32) {
+        const int b1 = std::min(nh, b0 + 32);
+        int order[32];
+        bool used[32] = {};
+        for (int e = b0; e < b1; ++e) order[e - b0] = e;
+        std::stable_sort(order, order + (b1 - b0), [&](int x, int y) {
+            return in_grp[static_cast<size_t>(x)].size() > in_grp[static_cast<size_t>(y)].size();
+        });
+        for (int i = 0; i < b1 - b0; ++i) {
+            const int e = order[i];
+            const auto& gs = in_grp[static_cast<size_t>(e)];
+            int best = -1;
+            long long bc = 0;
+            for (int j = 0; j < b1 - b0; ++j) {
+                if (used[j]) continue;
+                const int bank = (b0 + j) & 15;
+                long long c = 0;
+                for (int q : gs) {
+                    const long long k = cnt[static_cast<size_t>(q) * 16 + bank];
+                    c += 4 * k * k + k;
+                }
+                if (best < 0 || c < bc) { bc = c; best = j; }
+            }
+            used[best] = true;
+            pos[static_cast<size_t>(e)] = b0 + best;
+            const int bank = (b0 + best) & 15;
+            for (int q : gs) {
+                unsigned char& k = cnt[static_cast<size_t>(q) * 16 + bank];
+                if (k < 255) ++k;
+            }
+        }
+    }
+}
+
 // Instantiations of the single-reduction kernels by rows per thread, batch
 // mode and CTA size.
 template <bool BATCH, int NT, int KS = 0>
@@ -2466,8 +2672,20 @@ const void* fn_twolevel(int rmax)
          : rmax == 4 ? reinterpret_cast<const void*>(k_pcg64d<4>)
                      : reinterpret_cast<const void*>(k_pcg64d<8>);
 }
-const void* fn_cgcg_single(int rmax, int nt, int ks = 0)
+// rows per thread read from tensor memory by the one-CTA-per-SM kernel with
+// its first row in shared memory (0: that kernel has no such form)
+int cgcg_tmem_rows(int rmax) { return rmax == 2 ? 1 : rmax == 4 ? 3 : rmax == 8 ? 4 : 0; }
+const void* fn_cgcg_single(int rmax, int nt, int ks = 0, bool tmem = false)
 {
+    // every row of the thread in tensor memory (no shared-memory copy)
+    if (!ks && tmem && nt == 512 && (rmax == 2 || rmax == 4))
+        return rmax == 2 ? reinterpret_cast<const void*>(k_pcg64c<2, false, 512, 0, 2>)
+                         : reinterpret_cast<const void*>(k_pcg64c<4, false, 512, 0, 4>);
+    if (ks && tmem && nt == 512) {
+        return rmax == 2 ? reinterpret_cast<const void*>(k_pcg64c<2, false, 512, 1, 1>)
+             : rmax == 4 ? reinterpret_cast<const void*>(k_pcg64c<4, false, 512, 1, 3>)
+                         : reinterpret_cast<const void*>(k_pcg64c<8, false, 512, 1, 4>);
+    }
     if (ks) return nt == 256 ? fn_cgcg<false, 256, 1>(rmax) : fn_cgcg<false, 512, 1>(rmax);
     return nt == 256 ? fn_cgcg<false, 256>(rmax) : fn_cgcg<false, 512>(rmax);
 }
@@ -2653,7 +2871,7 @@ void PcgEngine::init(const HostModel& m, const uint8_t* nflag, const double* pfi
     variant = 1;
     nblocks = grid_for(reinterpret_cast<const void*>(k_pcg64<false>));
     const int rm[4] = {1, 2, 4, 8};
-    if (kernel_choice == 0 || kernel_choice == 3 || kernel_choice == 4) {
+    if (kernel_choice == 0 || kernel_choice == 3 || kernel_choice == 4 || kernel_choice == 10 || kernel_choice == 11) {
         const void* hc3[4] = {reinterpret_cast<const void*>(k_pcg64h<1>), reinterpret_cast<const void*>(k_pcg64h<2>),
                               reinterpret_cast<const void*>(k_pcg64h<4>), reinterpret_cast<const void*>(k_pcg64h<8>)};
         const int want = kernel_choice == 3 ? 3 : 4;
@@ -2671,13 +2889,13 @@ void PcgEngine::init(const HostModel& m, const uint8_t* nflag, const double* pfi
             if (g > nslices) g = nslices > 0 ? nslices : 1;
             const int per_cta = (nslices + g - 1) / g;
             if ((per_cta + nwarps - 1) / nwarps > rm[c]) continue;
-            // halo of every CTA: distinct columns of its slot range, sorted
+            // halo of every CTA: distinct columns of its slot range
             std::vector<int> hptr(static_cast<size_t>(g) + 1, 0), hidx;
             std::vector<unsigned short> lcol(static_cast<size_t>(nslots), 0);
             int hmax = 0;
             long long smax = 0;
             bool fits = true;
-            std::vector<int> cols;
+            std::vector<int> cols, hpos, hcols;
             for (int bb = 0; bb < g && fits; ++bb) {
                 const int sb = static_cast<int>(static_cast<long long>(bb) * nslices / g);
                 const int se = static_cast<int>(static_cast<long long>(bb + 1) * nslices / g);
@@ -2689,7 +2907,14 @@ void PcgEngine::init(const HostModel& m, const uint8_t* nflag, const double* pfi
                 for (long long t = a0; t < a1; ++t)
                     lcol[static_cast<size_t>(t)] = static_cast<unsigned short>(
                         std::lower_bound(cols.begin(), cols.end(), colp[static_cast<size_t>(t)]) - cols.begin());
-                hidx.insert(hidx.end(), cols.begin(), cols.end());
+                // the halo's order in shared memory: bank-spread
+                const int nh = static_cast<int>(cols.size());
+                bank_spread_halo(nh, lcol.data() + a0, P.slice_off.data(), P.slice_w.data(), sb, se, a0, hpos);
+                for (long long t = a0; t < a1; ++t)
+                    lcol[static_cast<size_t>(t)] = static_cast<unsigned short>(hpos[lcol[static_cast<size_t>(t)]]);
+                hcols.resize(cols.size());
+                for (int e = 0; e < nh; ++e) hcols[static_cast<size_t>(hpos[static_cast<size_t>(e)])] = cols[static_cast<size_t>(e)];
+                hidx.insert(hidx.end(), hcols.begin(), hcols.end());
                 hptr[static_cast<size_t>(bb) + 1] = static_cast<int>(hidx.size());
                 hmax = std::max(hmax, static_cast<int>(cols.size()));
                 smax = std::max(smax, a1 - a0);
@@ -2730,7 +2955,25 @@ void PcgEngine::init(const HostModel& m, const uint8_t* nflag, const double* pfi
             // the halo
             cgcg_ks = 0;
             cgcg_coef_off = 0;
-            if (want == 4) {
+            // tensor memory (one-CTA-per-SM kernel): 128 columns = 64 doubles
+            // per thread, the slots of a row padded to the widest slice of
+            // the mesh.  Where all the thread's rows fit, they all live there
+            // and no coefficients are copied into shared memory; otherwise
+            // the rows after the shared-memory one that fit.
+            cgcg_kt = 0;
+            cgcg_tm_w = 0;
+            int tm_tw = 0;
+            if (want == 4 && nt == 512 && kernel_choice != 10) {
+                int wmx = 0;
+                for (int q = 0; q < nslices; ++q) wmx = std::max(wmx, P.slice_w[static_cast<size_t>(q)]);
+                const int chw = rm[c] >= 4 ? 2 : 8;
+                tm_tw = (wmx + chw - 1) / chw * chw;
+                if (kernel_choice != 11 && (rm[c] == 2 || rm[c] == 4) && tm_tw > 0 && rm[c] * tm_tw <= 64) {
+                    cgcg_kt = rm[c];
+                    cgcg_tm_w = tm_tw;
+                }
+            }
+            if (want == 4 && cgcg_kt == 0) {
                 long long cmax = 0;
                 for (int bb = 0; bb < g; ++bb) {
                     const int sb = static_cast<int>(static_cast<long long>(bb) * nslices / g);
@@ -2753,6 +2996,14 @@ void PcgEngine::init(const HostModel& m, const uint8_t* nflag, const double* pfi
                 }
                 cudaGetLastError();
             }
+            // the one-CTA-per-SM kernel with its first row in shared memory
+            // keeps the coefficients of its next rows in the SM's tensor
+            // memory for the solve: 128 columns (64 doubles) per thread, the
+            // slots of a row padded to the widest slice of the mesh
+            if (cgcg_ks && tm_tw > 0 && cgcg_tmem_rows(rm[c]) * tm_tw <= 64) {
+                cgcg_kt = cgcg_tmem_rows(rm[c]);
+                cgcg_tm_w = tm_tw;
+            }
             // the one-CTA-per-SM kernel's rows' diagonal in shared memory
             // (64^3: 12.05 -> 11.95 us per iteration; in registers it was
             // slower)
@@ -2760,13 +3011,27 @@ void PcgEngine::init(const HostModel& m, const uint8_t* nflag, const double* pfi
             if (want == 4 && nt == 512) {
                 const size_t off = (cgcg_smem + 15) & ~static_cast<size_t>(15);
                 const size_t with = off + static_cast<size_t>(rm[c]) * nt * 8;
-                const void* fk = fn_cgcg_single(rm[c], nt, cgcg_ks);
+                const void* fk = fn_cgcg_single(rm[c], nt, cgcg_ks, cgcg_kt > 0);
                 int per2 = 0;
                 if (with <= 227 * 1024 && raise_smem_limit(fk, with) == cudaSuccess &&
                     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per2, fk, nt, with) == cudaSuccess &&
                     per2 * sms >= g) {
                     cgcg_smem = with;
                     cgcg_pds_off = static_cast<int>(off);
+                }
+                cudaGetLastError();
+            }
+            if (cgcg_kt > 0) {
+                // the tensor-memory kernel must hold the whole grid resident
+                // with one CTA per SM: each CTA takes all 512 columns, so a
+                // second CTA on the SM would wait for the first to finish
+                const void* fk = fn_cgcg_single(rm[c], nt, cgcg_ks, true);
+                int per2 = 0;
+                if (g > sms || !(raise_smem_limit(fk, cgcg_smem) == cudaSuccess &&
+                      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per2, fk, nt, cgcg_smem) == cudaSuccess &&
+                      per2 * sms >= g)) {
+                    cgcg_kt = 0;
+                    cgcg_tm_w = 0;
                 }
                 cudaGetLastError();
             }
@@ -2903,6 +3168,7 @@ void PcgEngine::init(const HostModel& m, const uint8_t* nflag, const double* pfi
     dev.xs_off = cgcg_xs_off;
     dev.coef_off = cgcg_coef_off;
     dev.pds_off = cgcg_pds_off;
+    dev.tm_w = cgcg_tm_w;
     dev.halo_parts = global_halo ? global_halo_parts : 0;
     dev.row_node = d_row_node;
 }
@@ -3007,7 +3273,7 @@ cbs3d_status PcgEngine::solve(double* pres, double* rhs1, double* pdiag, int pre
         fn = fn_mixed_single(rmax, nthreads);
         smem = mixed_smem;
     } else if (variant == 4) {
-        fn = fn_cgcg_single(rmax, nthreads, cgcg_ks);
+        fn = fn_cgcg_single(rmax, nthreads, cgcg_ks, cgcg_kt > 0);
         smem = cgcg_smem;
     }
     CoarseDev C = cdev;

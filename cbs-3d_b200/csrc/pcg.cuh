@@ -64,6 +64,8 @@ struct PcgDev {
                                  // memory: byte offset of that copy
     int pds_off;                 // one-CTA-per-SM CG-CG kernel: byte offset in shared memory of its
                                  // rows' diagonal (RMAX*threads doubles); 0: read from global memory
+    int tm_w;                    // CG-CG kernel with rows in tensor memory: slots per row there (the
+                                 // widest slice, rounded up to the kernel's load width)
 };
 
 class MgHierarchy;
@@ -142,6 +144,8 @@ public:
     int cgcg_xs_off = 0;     // where those rows start (0: kept in global memory)
     int cgcg_ks = 0;         // 1: the kernel reads its warps' first rows' coefficients from shared memory
     int cgcg_coef_off = 0;   // where they start
+    int cgcg_kt = 0;         // >0: that many rows per thread, after the shared-memory one, read from tensor memory
+    int cgcg_tm_w = 0;       // slots per row in tensor memory
     int cgcg_pds_off = 0;    // where the rows' diagonal starts in shared memory (0: global memory)
     size_t mixed_smem = 0;   // dynamic shared memory of the mixed-precision kernel
     bool mixed_ok = false;   // mixed precision runs on the FP32 kernel (else FP64)

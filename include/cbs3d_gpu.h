@@ -98,7 +98,11 @@ typedef struct cbs3d_options {
     int time_pcg;            /* time every PCG launch with CUDA events (no graph capture) */
     int pcg_kernel;          /* 0 automatic; 1 vectors in global memory, 2 register-resident rows,
                                 3 shared-memory halo, 4 halo + one grid sync per iteration,
-                                5 vectors in global memory + one grid sync per iteration */
+                                5 vectors in global memory + one grid sync per iteration,
+                                10 as 4 with no coefficients kept in tensor memory,
+                                11 as 4 with the first row per thread in shared memory and the
+                                next ones in tensor memory (0 and 4 keep every row in tensor
+                                memory where they all fit, else as 11) */
     int case_cache;          /* cbs3d_create_from_case: keep the parsed case in <case>.cbscache
                                 (keyed by every source file's size and time) and reuse it */
     int pcg_two_level;       /* extension: Jacobi plus a coarse correction on one aggregate of rows
@@ -144,7 +148,8 @@ typedef struct cbs3d_step_stats {
                                 3 shared-memory halo, 4 single-reduction (CG-CG),
                                 5 mixed FP32/FP64, 6 two-level (CG-CG + coarse correction),
                                 7 aggregation-multigrid preconditioned CG,
-                                8 global vectors, single-reduction (CG-CG) */
+                                8 global vectors, single-reduction (CG-CG),
+                                9 single-reduction (CG-CG) with coefficients in tensor memory */
 } cbs3d_step_stats;
 
 typedef struct cbs3d_ctx cbs3d_ctx;
