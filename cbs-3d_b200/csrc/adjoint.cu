@@ -35,6 +35,22 @@ constexpr double FD1 = 1.0 / 6.0, FD2 = 1.0 / 3.0;
 // nodes of face f (opposite local node f), as the forward kernels use them
 __constant__ int c_face[4][3] = {{2, 1, 3}, {2, 3, 0}, {0, 3, 1}, {0, 1, 2}};
 
+// Neumaier's compensated summation (host): the objective and the directional
+// derivatives are sums over every node, and a plain running sum over ~28,000
+// terms rounds by several ulp of the total, differently for J(f + h d) and
+// J(f - h d) -- at h = 1e-6 that rounding alone was comparable to the
+// difference being measured.  Compensated, the sum is rounded about once.
+struct CompSum {
+    double s = 0.0, c = 0.0;
+    void add(double x)
+    {
+        const double t = s + x;
+        c += std::fabs(s) >= std::fabs(x) ? (s - t) + x : (x - t) + s;
+        s = t;
+    }
+    double value() const { return s + c; }
+};
+
 __device__ __forceinline__ int nd(const int4& n, int a) { return a == 0 ? n.x : a == 1 ? n.y : a == 2 ? n.z : n.w; }
 __device__ __forceinline__ int fedge(uint8_t packed, int f) { return (packed >> (2 * f)) & 3; }
 
@@ -736,22 +752,22 @@ public:
         CUDA_OK(cudaMemcpyAsync(t.data(), c.S.temp, N * sizeof(double), cudaMemcpyDeviceToHost, st));
         CUDA_OK(cudaStreamSynchronize(st));
         c.check_status();
-        double J = 0.0;
-        for (size_t i = 0; i < N; ++i) J += w[i] * t[i];
+        CompSum J;
+        for (size_t i = 0; i < N; ++i) J.add(w[i] * t[i]);
         if (seed) {
             CUDA_OK(cudaMemcpyAsync(s0, w, N * sizeof(double), cudaMemcpyHostToDevice, st));
             CUDA_OK(cudaStreamSynchronize(st));
         }
-        return J;
+        return J.value();
     }
     double dot_plain(const double* w, const double* dvec)
     {
         std::vector<double> d(N);
         CUDA_OK(cudaMemcpyAsync(d.data(), dvec, N * sizeof(double), cudaMemcpyDeviceToHost, st));
         CUDA_OK(cudaStreamSynchronize(st));
-        double s = 0.0;
-        for (size_t i = 0; i < N; ++i) s += w[i] * d[i];
-        return s;
+        CompSum s;
+        for (size_t i = 0; i < N; ++i) s.add(w[i] * d[i]);
+        return s.value();
     }
 
     // J = 1/2 sum_i w_i |u_i|^2 of the current u; optionally lambda_N = w u into v0
@@ -761,9 +777,10 @@ public:
         CUDA_OK(cudaMemcpyAsync(u.data(), c.S.unkno, 3 * N * sizeof(double), cudaMemcpyDeviceToHost, st));
         CUDA_OK(cudaStreamSynchronize(st));
         c.check_status();
-        double J = 0.0;
+        CompSum Js;
         for (size_t i = 0; i < N; ++i)
-            J += 0.5 * w[i] * (u[3 * i] * u[3 * i] + u[3 * i + 1] * u[3 * i + 1] + u[3 * i + 2] * u[3 * i + 2]);
+            Js.add(0.5 * w[i] * (u[3 * i] * u[3 * i] + u[3 * i + 1] * u[3 * i + 1] + u[3 * i + 2] * u[3 * i + 2]));
+        const double J = Js.value();
         if (seed) {
             for (size_t i = 0; i < N; ++i)
                 for (int d = 0; d < 3; ++d) u[3 * i + d] *= w[i];
@@ -778,10 +795,10 @@ public:
         CUDA_OK(cudaMemcpyAsync(u.data(), c.S.unkno, 3 * N * sizeof(double), cudaMemcpyDeviceToHost, st));
         CUDA_OK(cudaMemcpyAsync(d.data(), dvec, 3 * N * sizeof(double), cudaMemcpyDeviceToHost, st));
         CUDA_OK(cudaStreamSynchronize(st));
-        double s = 0.0;
+        CompSum s;
         for (size_t i = 0; i < N; ++i)
-            s += w[i] * (u[3 * i] * d[3 * i] + u[3 * i + 1] * d[3 * i + 1] + u[3 * i + 2] * d[3 * i + 2]);
-        return s;
+            s.add(w[i] * (u[3 * i] * d[3 * i] + u[3 * i + 1] * d[3 * i + 1] + u[3 * i + 2] * d[3 * i + 2]));
+        return s.value();
     }
     double* alloc(size_t n)
     {
