@@ -327,6 +327,10 @@ def roofline(st, warm, nelem_fluid, npoin, mixed, n, pr, bound="l2"):
            "kernel_bytes_per_iteration": kb, "ebe_bytes_per_iteration": ebe_bytes(nelem_fluid, npoin, mixed),
            "iterations": its, "us_per_iteration": 1e6 * st.pcg_seconds / its if its > 0 else None,
            "launches": st.pcg_launches, "avg_launch_ms": 1e3 * st.pcg_seconds / max(st.pcg_launches, 1)}
+    if st.pcg_kernel == 9:
+        out["operator_storage"] = ("SELL coefficients held on chip in the SM's tensor memory for the whole solve "
+                                   "(tcgen05.ld every iteration); kernel_bytes_per_iteration still counts them, "
+                                   "with the vectors, as the algorithm's bytes")
     if bound == "l2":
         out["hbm_peak"] = hbm
         out["hbm_peak_source"] = hbm_kind
