@@ -2677,10 +2677,12 @@ const void* fn_twolevel(int rmax)
 int cgcg_tmem_rows(int rmax) { return rmax == 2 ? 1 : rmax == 4 ? 3 : rmax == 8 ? 4 : 0; }
 const void* fn_cgcg_single(int rmax, int nt, int ks = 0, bool tmem = false)
 {
-    // every row of the thread in tensor memory (no shared-memory copy)
-    if (!ks && tmem && nt == 512 && (rmax == 2 || rmax == 4))
+    // every row of the thread in tensor memory (no shared-memory copy); at
+    // eight rows the first four, the rest from L2
+    if (!ks && tmem && nt == 512)
         return rmax == 2 ? reinterpret_cast<const void*>(k_pcg64c<2, false, 512, 0, 2>)
-                         : reinterpret_cast<const void*>(k_pcg64c<4, false, 512, 0, 4>);
+             : rmax == 4 ? reinterpret_cast<const void*>(k_pcg64c<4, false, 512, 0, 4>)
+                         : reinterpret_cast<const void*>(k_pcg64c<8, false, 512, 0, 4>);
     if (ks && tmem && nt == 512) {
         return rmax == 2 ? reinterpret_cast<const void*>(k_pcg64c<2, false, 512, 1, 1>)
              : rmax == 4 ? reinterpret_cast<const void*>(k_pcg64c<4, false, 512, 1, 3>)
@@ -3002,6 +3004,12 @@ void PcgEngine::init(const HostModel& m, const uint8_t* nflag, const double* pfi
             // slots of a row padded to the widest slice of the mesh
             if (cgcg_ks && tm_tw > 0 && cgcg_tmem_rows(rm[c]) * tm_tw <= 64) {
                 cgcg_kt = cgcg_tmem_rows(rm[c]);
+                cgcg_tm_w = tm_tw;
+            }
+            // eight rows per thread where the shared-memory copy did not fit:
+            // the first four rows in tensor memory
+            if (!cgcg_ks && cgcg_kt == 0 && rm[c] == 8 && tm_tw > 0 && 4 * tm_tw <= 64) {
+                cgcg_kt = 4;
                 cgcg_tm_w = tm_tw;
             }
             // the one-CTA-per-SM kernel's rows' diagonal in shared memory

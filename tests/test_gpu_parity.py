@@ -307,7 +307,7 @@ def test_global_kernel_halo_in_parts(choice, kernel):
     assert rel_l2(pb, pa) <= RUN_TOL
 
 
-@pytest.mark.parametrize("n", [48, 64, 70])
+@pytest.mark.parametrize("n", [48, 64, 70, 72])
 def test_tensor_memory_coefficients_bitwise(n):
     """The register-resident single-reduction PCG reads its rows'
     coefficients from the SM's tensor memory (every row where they all fit,
@@ -315,7 +315,8 @@ def test_tensor_memory_coefficients_bitwise(n):
     (pcg_kernel=10): the same values enter the same products in the same
     order, so fields and iteration counts agree bit for bit.  48^3 runs two
     rows per thread, 64^3 (the bench mesh) four, 70^3 eight (the first in
-    shared memory, the next four in tensor memory, the rest from L2)."""
+    shared memory, the next four in tensor memory, the rest from L2), 72^3
+    eight without the shared-memory copy (the first four in tensor memory)."""
     from cbs3d import cases
     gpu = _gpu()
     case = cases.cavity(n, re=400.0, ntime=10 ** 6, jitter=0.15, seed=1234)
