@@ -2647,6 +2647,32 @@ void bank_spread_halo(int nh, const unsigned short* lc, const long long* slice_o
     }
 }
 
+// Shared-memory wavefronts of the neighbour gathers of slices sb..se-1 with
+// the halo entries at `pos`: per slot and half warp, the largest number of
+// distinct entries sharing a bank pair (at least one).
+long long gather_wavefronts(const unsigned short* lc, const long long* slice_off, const int* slice_w, int sb, int se,
+                            long long a0, const std::vector<int>& pos)
+{
+    long long w = 0;
+    for (int s = sb; s < se; ++s)
+        for (int u = 0; u < slice_w[s]; ++u)
+            for (int hw = 0; hw < 2; ++hw) {
+                int seen[16], nseen = 0, cnt[16] = {};
+                for (int l = 16 * hw; l < 16 * hw + 16; ++l) {
+                    const int p = pos[lc[slice_off[s] - a0 + 32 * u + l]];
+                    bool dup = false;
+                    for (int q = 0; q < nseen; ++q) dup = dup || seen[q] == p;
+                    if (dup) continue;
+                    seen[nseen++] = p;
+                    ++cnt[p & 15];
+                }
+                int m = 1;
+                for (int b = 0; b < 16; ++b) m = std::max(m, cnt[b]);
+                w += m;
+            }
+    return w;
+}
+
 // Instantiations of the single-reduction kernels by rows per thread, batch
 // mode and CTA size.
 template <bool BATCH, int NT, int KS = 0>
@@ -3705,3 +3731,26 @@ void PcgBatch::finish(int k, double* pres, cudaStream_t st)
 }
 
 }  // namespace cbs3d
+
+extern "C" cbs3d_status cbs3d_probe_halo_placement(int nh, int nslices, const long long* slice_off, const int* slice_w,
+                                                   const unsigned short* lc, int* pos, long long* wavefronts)
+{
+    try {
+        if (nh < 1 || nh > 65535 || nslices < 1 || !slice_off || !slice_w || !lc || !pos || !wavefronts)
+            return CBS3D_INVALID_INPUT;
+        if (slice_off[0] != 0) return CBS3D_INVALID_INPUT;
+        for (int q = 0; q < nslices; ++q)
+            if (slice_w[q] < 0 || slice_off[q + 1] - slice_off[q] != 32LL * slice_w[q]) return CBS3D_INVALID_INPUT;
+        for (long long t = 0; t < slice_off[nslices]; ++t)
+            if (lc[t] >= nh) return CBS3D_INVALID_INPUT;
+        std::vector<int> id(static_cast<size_t>(nh)), pv;
+        for (int e = 0; e < nh; ++e) id[static_cast<size_t>(e)] = e;
+        wavefronts[0] = cbs3d::gather_wavefronts(lc, slice_off, slice_w, 0, nslices, 0, id);
+        cbs3d::bank_spread_halo(nh, lc, slice_off, slice_w, 0, nslices, 0, pv);
+        wavefronts[1] = cbs3d::gather_wavefronts(lc, slice_off, slice_w, 0, nslices, 0, pv);
+        for (int e = 0; e < nh; ++e) pos[e] = pv[static_cast<size_t>(e)];
+        return CBS3D_OK;
+    } catch (...) {
+        return CBS3D_INTERNAL;
+    }
+}

@@ -418,6 +418,18 @@ cbs3d_status cbs3d_coarse_inverse(int device, int g, const double* a, double* ai
 cbs3d_status cbs3d_probe_bandwidth(int device, long long bytes, int passes, int mode, double* gbs);
 cbs3d_status cbs3d_probe_allreduce(int device, int iters, double* us_per_allreduce);
 
+/* Halo placement probe (no reference counterpart; host only, touches no
+ * device).  For one CTA's SELL-32 slices -- slice q holds slice_w[q] slots
+ * per row at slice_off[q] (slice_off[0] = 0, slot u of lane l at
+ * slice_off[q] + 32*u + l), lc giving each slot's halo entry 0..nh-1 in
+ * column order -- returns in pos[nh] the shared-memory position the PCG
+ * engine gives each halo entry (a permutation within every aligned block of
+ * 32 positions, spreading the warps' gathers over the bank pairs), and in
+ * wavefronts[0..1] the gathers' shared-memory wavefronts under a half-warp
+ * bank-pair model with the entries in column order and as placed. */
+cbs3d_status cbs3d_probe_halo_placement(int nh, int nslices, const long long* slice_off, const int* slice_w,
+                                        const unsigned short* lc, int* pos, long long* wavefronts);
+
 #ifdef __cplusplus
 }
 #endif

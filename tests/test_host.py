@@ -250,3 +250,50 @@ def test_integration_snippet_is_the_compiled_backend():
     block = re.search(r"```cpp\n(.*?)```", doc, re.S).group(1)
     inc = open(os.path.join(root, "oracle", "gpu_pressure_solver.inc")).read()
     assert block.strip() in inc
+
+
+def _gather_wavefronts(lc, slice_w, pos):
+    """Half-warp bank-pair model of the neighbour gathers: per slot and half
+    warp, the largest number of distinct halo entries sharing a bank pair."""
+    w, off = 0, 0
+    for width in slice_w:
+        for u in range(width):
+            for hw in range(2):
+                p = {int(pos[lc[off + 32 * u + l]]) for l in range(16 * hw, 16 * hw + 16)}
+                cnt = np.bincount(np.array(sorted(p)) % 16, minlength=16)
+                w += max(1, int(cnt.max()))
+        off += 32 * width
+    return w
+
+
+def test_halo_placement_probe():
+    """The PCG engine's shared-memory placement of a CTA's halo (host only):
+    a permutation that keeps every aligned block of 32 positions (so the
+    staging loads read the same L2 sectors) and does not raise the gathers'
+    bank-pair wavefronts; on random slot columns it lowers them.  The probe's
+    wavefront counts match the model recomputed here."""
+    from cbs3d import gpu
+    L = gpu.lib()
+    L.cbs3d_probe_halo_placement.restype = ctypes.c_int
+    rng = np.random.default_rng(7)
+    nh, widths = 1000, [12] * 20 + [9] * 12
+    slice_w = np.array(widths, dtype=np.int32)
+    slice_off = np.concatenate([[0], np.cumsum(32 * slice_w)]).astype(np.int64)
+    lc = rng.integers(0, nh, size=int(slice_off[-1])).astype(np.uint16)
+    pos = np.empty(nh, dtype=np.int32)
+    wf = np.zeros(2, dtype=np.int64)
+    P = ctypes.c_void_p
+    rc = L.cbs3d_probe_halo_placement(nh, len(widths), P(slice_off.ctypes.data), P(slice_w.ctypes.data),
+                                      P(lc.ctypes.data), P(pos.ctypes.data), P(wf.ctypes.data))
+    assert rc == 0
+    assert sorted(pos.tolist()) == list(range(nh))
+    for b0 in range(0, nh, 32):
+        assert set(pos[b0:b0 + 32].tolist()) == set(range(b0, min(nh, b0 + 32)))
+    assert wf[0] == _gather_wavefronts(lc, widths, np.arange(nh))
+    assert wf[1] == _gather_wavefronts(lc, widths, pos)
+    assert wf[1] < wf[0]
+    # a slot naming an entry past the halo is rejected
+    bad = lc.copy()
+    bad[5] = nh
+    assert L.cbs3d_probe_halo_placement(nh, len(widths), P(slice_off.ctypes.data), P(slice_w.ctypes.data),
+                                        P(bad.ctypes.data), P(pos.ctypes.data), P(wf.ctypes.data)) != 0
