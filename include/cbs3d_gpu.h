@@ -420,7 +420,8 @@ cbs3d_status cbs3d_probe_allreduce(int device, int iters, double* us_per_allredu
 
 /* Halo placement probe (no reference counterpart; host only, touches no
  * device).  For one CTA's SELL-32 slices -- slice q holds slice_w[q] slots
- * per row at slice_off[q] (slice_off[0] = 0, slot u of lane l at
+ * per row at slice_off[q] (nslices+1 offsets, slice_off[0] = 0 and
+ * slice_off[q+1] = slice_off[q] + 32*slice_w[q]; slot u of lane l at
  * slice_off[q] + 32*u + l), lc giving each slot's halo entry 0..nh-1 in
  * column order -- returns in pos[nh] the shared-memory position the PCG
  * engine gives each halo entry (a permutation within every aligned block of
