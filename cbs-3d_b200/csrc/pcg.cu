@@ -899,7 +899,8 @@ __device__ __forceinline__ bool grid_allreduce_v(double (&v)[NV], const PcgDev& 
     }
     __syncthreads();
     // no barrier after these reads: so is rewritten only after the next
-    // call's second barrier, which every thread reaches after reading it
+    // call's third barrier, and every thread reads it before it arrives at
+    // that call's first
 #pragma unroll
     for (int q = 0; q < NV; ++q) out[q] = so[q];
     return ok;
